@@ -1,0 +1,298 @@
+"""TEST INFRASTRUCTURE: CPU oracles of the projector hot path.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may import this package.  It is the checker, never the product
+path: ``nefct_b200`` does not import it and has no CPU fallback.
+
+Two layers:
+
+* ``liboracle.so`` -- a plain-C restatement of the reference's slab-split
+  Siddon walk, its cone-beam and LOR drivers, the pixel_3d voxel-driven
+  backprojection, the cpp/deform warp, and an exact FP64 Siddon
+  (``nefct_oracle.c``, file:line citations inside).
+* ``_ref/libnefct_ref.so`` -- the reference's own device routines compiled as
+  host C++ from the reference sources (``ref_shim.cc``, ``Makefile``).  Used to
+  pin the restatement and as the "reference" CPU baseline.  Present only when
+  it was built (it needs the reference checkout at build time).
+
+The FDK filter restatement of the MATLAB code lives in ``oracle.fdk``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(HERE, "liboracle.so")
+_REF = os.path.join(HERE, "_ref", "libnefct_ref.so")
+
+TIE_GE, SKIP_SHORT, INV_L2, Q5_TRIPLE_L = 1, 2, 4, 8
+CB_FWD = TIE_GE | INV_L2
+CB_BP = SKIP_SHORT
+LOR_FWD = SKIP_SHORT | INV_L2 | Q5_TRIPLE_L
+LOR_BP = SKIP_SHORT
+
+
+class Grid(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("cx", C.c_float), ("cy", C.c_float), ("cz", C.c_float),
+                ("sx", C.c_float), ("sy", C.c_float), ("sz", C.c_float)]
+
+
+def build(ref: str | None = None) -> None:
+    """Run oracle/Makefile (C restatement, plus oracle/_ref when the
+    reference checkout is present)."""
+    env = dict(os.environ)
+    if ref:
+        env["REF"] = ref
+    subprocess.run(["make", "-s", "-C", HERE], check=True, env=env)
+
+
+_lib = None
+_ref = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        _lib = C.CDLL(_LIB)
+    return _lib
+
+
+def have_ref() -> bool:
+    return os.path.exists(_REF)
+
+
+def ref() -> C.CDLL:
+    global _ref
+    if _ref is None:
+        if not os.path.exists(_REF):
+            raise FileNotFoundError("oracle/_ref/libnefct_ref.so was not built")
+        _ref = C.CDLL(_REF)
+    return _ref
+
+
+def _p(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.flags.c_contiguous
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def grid(shape, center=(0.0, 0.0, 0.0), size=None) -> Grid:
+    """shape is (nx, ny, nz); the volume array is [nz][ny][nx] (x fastest)."""
+    nx, ny, nz = shape
+    if size is None:
+        size = (float(nx), float(ny), float(nz))
+    return Grid(nx, ny, nz, *[float(c) for c in center], *[float(s) for s in size])
+
+
+def trig(angles, use_cosf: bool) -> tuple[np.ndarray, np.ndarray]:
+    a = _f32(angles)
+    cs = np.empty_like(a)
+    sn = np.empty_like(a)
+    L = lib()
+    L.or_trig_f32(_p(a), C.c_int(a.size), C.c_int(int(use_cosf)), _p(cs), _p(sn))
+    return cs, sn
+
+
+def cb_forward(g: Grid, vol, angles, src_iso, src_det, na, da, ai, nb, db, bi, *, cyl=False,
+               flags=CB_FWD, off=None, use_cosf=False, f64=False):
+    """Sinogram [nv][nb][na] of vol [nz][ny][nx]; returns (sino, intersections)."""
+    L = lib()
+    nv = len(angles)
+    if f64:
+        a = _f64(angles)
+        cs, sn = np.cos(a), np.sin(a)
+        v = _f64(vol)
+        out = np.zeros((nv, nb, na), np.float64)
+        fn, cv, conv = L.or_cb_forward_f64, C.c_double, _f64
+    else:
+        cs, sn = trig(angles, use_cosf)
+        v = _f32(vol)
+        out = np.zeros((nv, nb, na), np.float32)
+        fn, cv, conv = L.or_cb_forward_f32, C.c_float, _f32
+    fn.restype = C.c_longlong
+    o = None if off is None else conv(off)
+    cnt = fn(C.byref(g), _p(v), _p(conv(cs)), _p(conv(sn)), _p(o), C.c_int(nv), cv(src_iso),
+             cv(src_det), C.c_int(na), cv(da), cv(ai), C.c_int(nb), cv(db), cv(bi),
+             C.c_int(int(cyl)), C.c_uint(flags), _p(out))
+    return out, int(cnt)
+
+
+def cb_backward(g: Grid, sino, angles, src_iso, src_det, na, da, ai, nb, db, bi, *, cyl=False,
+                flags=CB_BP, q8=False, off=None, use_cosf=False, f64=False):
+    """Scatter a [nv][nb][na] sinogram into a new [nz][ny][nx] volume."""
+    L = lib()
+    nv = len(angles)
+    shape = (g.nz, g.ny, g.nx)
+    if f64:
+        a = _f64(angles)
+        cs, sn = np.cos(a), np.sin(a)
+        s = _f64(sino)
+        out = np.zeros(shape, np.float64)
+        fn, cv, conv = L.or_cb_backward_f64, C.c_double, _f64
+    else:
+        cs, sn = trig(angles, use_cosf)
+        s = _f32(sino)
+        out = np.zeros(shape, np.float32)
+        fn, cv, conv = L.or_cb_backward_f32, C.c_float, _f32
+    o = None if off is None else conv(off)
+    fn(C.byref(g), _p(s), _p(conv(cs)), _p(conv(sn)), _p(o), C.c_int(nv), cv(src_iso), cv(src_det),
+       C.c_int(na), cv(da), cv(ai), C.c_int(nb), cv(db), cv(bi), C.c_int(int(cyl)),
+       C.c_uint(flags), C.c_int(int(q8)), _p(out))
+    return out
+
+
+def cb_exact(g: Grid, vol, angles, src_iso, src_det, na, da, ai, nb, db, bi, *, cyl=False,
+             inv_l2=True, off=None):
+    """Exact FP64 line integrals (classical Siddon) of every cone-beam ray."""
+    L = lib()
+    nv = len(angles)
+    out = np.zeros((nv, nb, na), np.float64)
+    o = None if off is None else _f64(off)
+    L.or_cb_exact_f64(C.byref(g), _p(_f64(vol)), _p(_f64(angles)), _p(o), C.c_int(nv),
+                      C.c_double(src_iso), C.c_double(src_det), C.c_int(na), C.c_double(da),
+                      C.c_double(ai), C.c_int(nb), C.c_double(db), C.c_double(bi),
+                      C.c_int(int(cyl)), C.c_int(int(inv_l2)), _p(out))
+    return out
+
+
+def lor_forward(g: Grid, vol, lors, flags=LOR_FWD):
+    L = lib()
+    lr = _f32(lors)
+    n = lr.shape[1]
+    out = np.zeros(n, np.float32)
+    L.or_lor_forward_f32.restype = C.c_longlong
+    cnt = L.or_lor_forward_f32(C.byref(g), _p(_f32(vol)), _p(lr), C.c_longlong(n), C.c_uint(flags), _p(out))
+    return out, int(cnt)
+
+
+def lor_backward(g: Grid, vals, lors, flags=LOR_BP):
+    L = lib()
+    lr = _f32(lors)
+    out = np.zeros((g.nz, g.ny, g.nx), np.float32)
+    L.or_lor_backward_f32(C.byref(g), _p(_f32(vals)), _p(lr), C.c_longlong(lr.shape[1]),
+                          C.c_uint(flags), _p(out))
+    return out
+
+
+def pixel_backproject(sino, angles, shape, corner, size, src_iso, src_det, na, da, ai, nb, db, bi,
+                      *, cyl=False, fdk=False, f64=False):
+    """Voxel-driven bilinear backprojection (pixel_3d), optional FDK weight."""
+    L = lib()
+    nx, ny, nz = shape
+    nv = len(angles)
+    if f64:
+        conv, cv, fn, dt = _f64, C.c_double, L.or_pixel_backproject_f64, np.float64
+    else:
+        conv, cv, fn, dt = _f32, C.c_float, L.or_pixel_backproject_f32, np.float32
+    out = np.zeros((nz, ny, nx), dt)
+    fn(_p(conv(sino)), _p(conv(angles)), C.c_int(nv), C.c_int(nx), C.c_int(ny), C.c_int(nz),
+       _p(conv(corner)), _p(conv(size)), cv(src_iso), cv(src_det), C.c_int(na), cv(da), cv(ai),
+       C.c_int(nb), cv(db), cv(bi), C.c_int(int(cyl)), C.c_int(int(fdk)), _p(out))
+    return out
+
+
+def deform(img, mx, my, mz, f64=False):
+    L = lib()
+    conv = _f64 if f64 else _f32
+    img = conv(img)
+    nz, ny, nx = img.shape
+    out = np.zeros_like(img)
+    fn = L.or_deform_f64 if f64 else L.or_deform_f32
+    fn(_p(img), _p(conv(mx)), _p(conv(my)), _p(conv(mz)), C.c_int(nx), C.c_int(ny), C.c_int(nz), _p(out))
+    return out
+
+
+# ---------------- the reference itself, compiled for the host ----------------
+
+def ref_cb_forward(g: Grid, vol, angles, SID, SAD, na, da, ai, nb, db, bi, *, cyl=False, f64=False):
+    """siddon_3d project_flat/project_cyli (kernel naming: SID = source to
+    axis, SAD = source to detector)."""
+    R = ref()
+    nv = len(angles)
+    if f64:
+        conv, cv, fn, dt = _f64, C.c_double, R.ref_s3d_project_f64, np.float64
+    else:
+        conv, cv, fn, dt = _f32, C.c_float, R.ref_s3d_project, np.float32
+    out = np.zeros((nv, nb, na), dt)
+    fn(C.c_int(int(cyl)), _p(conv(vol)), C.c_int(g.nx), C.c_int(g.ny), C.c_int(g.nz),
+       cv(g.cx), cv(g.cy), cv(g.cz), cv(g.sx), cv(g.sy), cv(g.sz), _p(conv(angles)), C.c_int(na),
+       C.c_int(nb), C.c_int(nv), cv(SID), cv(SAD), cv(da), cv(ai), cv(db), cv(bi), _p(out))
+    return out
+
+
+def ref_cb_backward(g: Grid, sino, angles, SID, SAD, na, da, ai, nb, db, bi, *, cyl=False, f64=False):
+    R = ref()
+    nv = len(angles)
+    if f64:
+        conv, cv, fn, dt = _f64, C.c_double, R.ref_s3d_backproject_f64, np.float64
+    else:
+        conv, cv, fn, dt = _f32, C.c_float, R.ref_s3d_backproject, np.float32
+    s = conv(sino).reshape(-1)
+    if cyl:
+        # Q8 indexing reaches ia + iv*na + ib*na*nb; pad with zeros past the end
+        need = (na - 1) + (nv - 1) * na + (nb - 1) * na * nb + 1
+        if need > s.size:
+            s = np.concatenate([s, np.zeros(need - s.size, s.dtype)])
+    out = np.zeros((g.nz, g.ny, g.nx), dt)
+    fn(C.c_int(int(cyl)), _p(s), C.c_int(g.nx), C.c_int(g.ny), C.c_int(g.nz), cv(g.cx), cv(g.cy),
+       cv(g.cz), cv(g.sx), cv(g.sy), cv(g.sz), _p(conv(angles)), C.c_int(na), C.c_int(nb), C.c_int(nv),
+       cv(SID), cv(SAD), cv(da), cv(ai), cv(db), cv(bi), _p(out))
+    return out
+
+
+def ref_lor_forward(g: Grid, vol, lors):
+    R = ref()
+    lr = _f32(lors)
+    n = lr.shape[1]
+    out = np.zeros(n, np.float32)
+    R.ref_lor_project(_p(lr), C.c_longlong(n), _p(_f32(vol)), C.c_int(g.nx), C.c_int(g.ny),
+                      C.c_int(g.nz), C.c_float(g.cx), C.c_float(g.cy), C.c_float(g.cz),
+                      C.c_float(g.sx), C.c_float(g.sy), C.c_float(g.sz), _p(out))
+    return out
+
+
+def ref_lor_backward(g: Grid, vals, lors):
+    R = ref()
+    lr = _f32(lors)
+    out = np.zeros((g.nz, g.ny, g.nx), np.float32)
+    R.ref_lor_backproject(_p(lr), C.c_longlong(lr.shape[1]), _p(_f32(vals)), C.c_int(g.nx),
+                          C.c_int(g.ny), C.c_int(g.nz), C.c_float(g.cx), C.c_float(g.cy),
+                          C.c_float(g.cz), C.c_float(g.sx), C.c_float(g.sy), C.c_float(g.sz), _p(out))
+    return out
+
+
+def ref_pixel_backproject(sino, angles, shape, corner, size, SID, SAD, na, da, ai, nb, db, bi, *, cyl=False):
+    R = ref()
+    nx, ny, nz = shape
+    out = np.zeros((nz, ny, nx), np.float32)
+    R.ref_pixel_backproject(C.c_int(int(cyl)), _p(_f32(sino)), C.c_int(nx), C.c_int(ny), C.c_int(nz),
+                            _p(_f32(corner)), _p(_f32(size)), _p(_f32(angles)), C.c_int(na),
+                            C.c_int(nb), C.c_int(len(angles)), C.c_float(SID), C.c_float(SAD),
+                            C.c_float(da), C.c_float(ai), C.c_float(db), C.c_float(bi), _p(out))
+    return out
+
+
+def ref_deform(img, mx, my, mz):
+    R = ref()
+    img = _f32(img)
+    nz, ny, nx = img.shape
+    out = np.zeros_like(img)
+    R.ref_deform(_p(img), _p(_f32(mx)), _p(_f32(my)), _p(_f32(mz)), C.c_int(nx), C.c_int(ny),
+                 C.c_int(nz), _p(out))
+    return out

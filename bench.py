@@ -1,0 +1,332 @@
+"""Benchmark: cone-beam forward projection + exact adjoint on one B200.
+
+Workload (default, the FDK configuration's scanner): 256^3 float32 volume of
+1 mm voxels holding 30 seeded ellipsoids, 360 views over 360 deg, flat
+detector 512 x 384 at 1.2 mm, source-axis 600 mm, source-detector 1200 mm.
+One step = forward projection (reference slab-split weights) of the volume
+plus the exact transpose of the sinogram (what one autograd
+forward+backward of the projector does).
+
+Metric: ray-voxel intersections per second, forward + adjoint (I
+intersections each, I counted exactly by the count kernel).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+N > 1: launched by torchrun, one rank per GPU; every rank runs its own scan
+(independent seeded phantom), no collective on the data path ("weak").
+Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CFG = dict(n=256, voxel=1.0, ellipsoids=30, seed=2, nv=360, na=512, nb=384, pixel=1.2,
+           src_iso=600.0, src_det=1200.0)
+METRIC = "ray-voxel intersections/s (forward + adjoint)"
+UNIT = "intersections/s"
+
+
+def workload_name(c=CFG):
+    return (f"cone-beam fwd+adjoint {c['n']}^3 @{c['voxel']}mm, {c['ellipsoids']} ellipsoids, {c['nv']} views, "
+            f"{c['na']}x{c['nb']} @{c['pixel']}mm, SID {c['src_iso']:.0f} / SDD {c['src_det']:.0f} mm")
+
+
+def config_dict(extra=None):
+    d = {"workload": workload_name(), "volume": [CFG["n"]] * 3, "views": CFG["nv"],
+         "detector": [CFG["na"], CFG["nb"]], "l2": "flushed between timed steps (256 MiB write)",
+         "parallelism": "independent scan per GPU"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+def angles():
+    return np.linspace(0, 2 * np.pi, CFG["nv"], endpoint=False).astype(np.float32)
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup(n_gpus):
+    import torch
+    import torch.distributed as dist
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        rank, local = dist.get_rank(), int(os.environ.get("LOCAL_RANK", "0"))
+    else:
+        rank, local = 0, 0
+    torch.cuda.set_device(local)
+    return rank, ws, local
+
+
+def max_over_ranks(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    import torch
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+# ---------------- CPU baseline (the reference, compiled for the host) ----------------
+
+def cpu_sample(views_per_step, steps, warmup=0, seed=2):
+    """Times the reference's own forward + backprojection (oracle/_ref, or the
+    oracle restatement when the reference build is absent) on a subset of
+    views of the workload, all host threads.  Returns (I/s, kind, cores, sample)."""
+    import oracle
+    import nefct_b200 as nb
+    import torch
+    kind = "reference" if oracle.have_ref() else "port"
+    n = CFG["n"]
+    vol = nb.ellipsoid_phantom(n, nb.random_ellipsoids(CFG["ellipsoids"], seed),
+                               device="cuda" if torch.cuda.is_available() else None)
+    vol = vol.permute(2, 1, 0).contiguous().cpu().numpy()
+    g = oracle.grid((n, n, n), (0, 0, 0), (n * CFG["voxel"],) * 3)
+    ang = angles()
+    a = (CFG["src_iso"], CFG["src_det"], CFG["na"], CFG["pixel"], 0.5, CFG["nb"], CFG["pixel"], 0.5)
+    tot_i, tot_t = 0, 0.0
+    for s in range(warmup + steps):
+        idx = [(s * views_per_step + k) * 37 % CFG["nv"] for k in range(views_per_step)]
+        sub = ang[idx]
+        _, cnt = oracle.cb_forward(g, vol, sub, *a)        # exact count of the sample
+        t0 = time.perf_counter()
+        if kind == "reference":
+            sino = oracle.ref_cb_forward(g, vol, sub, *a)
+            oracle.ref_cb_backward(g, sino, sub, *a)
+        else:
+            sino, _ = oracle.cb_forward(g, vol, sub, *a, use_cosf=True)
+            oracle.cb_backward(g, sino, sub, *a, use_cosf=True)
+        dt = time.perf_counter() - t0
+        if s >= warmup:
+            tot_i += 2 * cnt
+            tot_t += dt
+    cores = os.cpu_count() or 1
+    sample = (f"{views_per_step} views per step ({steps} steps) of the workload: reference siddon_3d "
+              f"project_flat + backproject_flat device code compiled as host C++ (-O3, OpenMP)")
+    return tot_i / tot_t, kind, cores, sample
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU path on the host cores."""
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    views = 2
+    v, kind, cores, sample = cpu_sample(views, args.steps, args.warmup)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_dict({"ranks_running": 1 if ws > 1 else 1}),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------- GPU arm ----------------
+
+def run_gpu(args):
+    import torch
+    import nefct_b200 as nb
+    from nefct_b200 import ops
+
+    rank, ws, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", local)
+    n = CFG["n"]
+    geom = nb.ConeBeam((n, n, n), angles(), CFG["src_iso"], CFG["src_det"], CFG["na"], CFG["pixel"], CFG["nb"],
+                       CFG["pixel"], size=(n * CFG["voxel"],) * 3)
+    vol = nb.ellipsoid_phantom(n, nb.random_ellipsoids(CFG["ellipsoids"], CFG["seed"] + rank), device=dev)
+    vol = vol.permute(2, 1, 0).contiguous()
+    inter = ops.cb_count_intersections(geom, 0, device=dev)
+    rays = CFG["nv"] * CFG["na"] * CFG["nb"]
+    sino = torch.empty(geom.sino_shape, device=dev)
+    back = torch.empty(geom.vol_shape, device=dev)
+    flush = torch.empty(256 * 2 ** 20 // 4, device=dev)
+
+    def step():
+        ops.cb_forward(vol, geom, 0, out=sino)
+        ops.cb_backward(sino, geom, 0, out=back)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(ws)
+    with ClockSampler(local) as clk:
+        wall0 = time.perf_counter()
+        for e0, e1, e2 in ev:
+            flush.fill_(1.0)                                   # L2 flush, outside the timed events
+            e0.record()
+            ops.cb_forward(vol, geom, 0, out=sino)
+            e1.record()
+            ops.cb_backward(sino, geom, 0, out=back)
+            e2.record()
+        barrier(ws)
+        wall = time.perf_counter() - wall0
+    t_fwd = sum(a.elapsed_time(b) for a, b, _ in ev) / 1e3
+    t_bwd = sum(b.elapsed_time(c) for _, b, c in ev) / 1e3
+    t_step = max_over_ranks(t_fwd + t_bwd, ws)
+    value = ws * args.steps * 2 * inter / t_step
+
+    # e2e through the public op API with pinned host buffers: H2D volume,
+    # forward + adjoint, D2H of the adjoint volume, every step
+    h_in = torch.empty(geom.vol_shape, pin_memory=True)
+    h_in.copy_(vol.cpu())
+    h_out = torch.empty(geom.vol_shape, pin_memory=True)
+    d_in = torch.empty_like(vol)
+    for _ in range(max(1, args.warmup)):
+        d_in.copy_(h_in, non_blocking=True)
+        step()
+    barrier(ws)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        d_in.copy_(h_in, non_blocking=True)
+        ops.cb_forward(d_in, geom, 0, out=sino)
+        ops.cb_backward(sino, geom, 0, out=back)
+        h_out.copy_(back, non_blocking=True)
+    e1.record()
+    barrier(ws)
+    t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3, ws)
+    e2e = ws * args.steps * 2 * inter / t_e2e
+    vbytes = int(vol.numel() * 4)
+
+    # roofline of the dominant op (forward or adjoint) on its algorithmic bytes
+    peak, peak_kind = load_peaks()
+    fwd_s, bwd_s = t_fwd / args.steps, t_bwd / args.steps
+    if bwd_s >= fwd_s:
+        dom, dom_t, alg = "cb_backward_kernel", bwd_s, 8 * inter + 4 * rays
+    else:
+        dom, dom_t, alg = "cb_forward_kernel", fwd_s, 4 * inter + 4 * rays
+    achieved = alg / dom_t / 1e9
+    traffic = load_traffic().get(dom)
+
+    extras = {"intersections_per_direction": inter, "rays": rays,
+              "forward_ms": 1e3 * fwd_s, "adjoint_ms": 1e3 * bwd_s,
+              "forward_intersections_per_s": inter / fwd_s, "adjoint_intersections_per_s": inter / bwd_s,
+              "wall_s_timed_loop": wall}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        v, kind, cores, sample = cpu_sample(2, 3)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * t_step / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ellipsoid phantom)",
+                "config": config_dict(),
+                "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "peak_source": peak_kind,
+                             "algorithmic_bytes": alg, "traffic": traffic},
+                "cpu_baseline": cpu,
+                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": vbytes, "d2h_bytes_per_step": vbytes},
+                "gpu_launches": 4 * args.steps,
+                "clocks": clk.summary(), "extras": extras}
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

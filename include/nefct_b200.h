@@ -1,0 +1,196 @@
+/*
+ * nefct_b200 -- C ABI of the B200 (sm_100a) projector library.
+ *
+ * Replaces the TensorFlow custom ops of bill52547/CT-NEF (package `nefct`)
+ * on the projector hot path: the cone-beam ray-driven ("Siddon") forward
+ * projector, its exact transpose, the reference's own backprojection, the
+ * LOR projector pair, FDK filtering and voxel-driven backprojection, and the
+ * trilinear deformation warp.
+ *
+ * Conventions (all entry points):
+ *  - plain pointers and sizes; device pointers unless stated "host";
+ *  - the caller owns every buffer; temporaries live in a caller-provided
+ *    workspace whose size a *_workspace_bytes() query returns;
+ *  - work is enqueued on `stream` (a cudaStream_t, NULL = legacy default
+ *    stream) with no host synchronisation and no host round trip;
+ *  - outputs are fully written (zeroed first where the op accumulates);
+ *  - every call returns an nefct_status; nefct_last_error() gives the
+ *    calling thread's message for the last failure.  No call aborts or traps;
+ *  - volumes are float [nz][ny][nx] (x fastest), sinograms [nv][nb][na]
+ *    (detector column a fastest), the reference's device layouts.
+ */
+#ifndef NEFCT_B200_H
+#define NEFCT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t nefct_status;
+#define NEFCT_OK              0
+#define NEFCT_ERR_INVALID     1  /* bad argument, shape or geometry */
+#define NEFCT_ERR_CUDA        2  /* a CUDA runtime call or launch failed */
+#define NEFCT_ERR_WORKSPACE   3  /* workspace missing or too small */
+#define NEFCT_ERR_TIMEOUT     4  /* a bounded device-side wait gave up */
+#define NEFCT_ERR_UNSUPPORTED 5  /* valid request this build does not implement */
+
+const char *nefct_version(void);
+const char *nefct_status_string(nefct_status st);
+const char *nefct_last_error(void);
+
+/* Voxel grid: nx*ny*nz voxels of a box of extent (sx, sy, sz) centred on
+ * (cx, cy, cz).  Same meaning as the reference ops' grid/center/size inputs
+ * (nefct/cc/siddon_3d/siddon.cc:13-15; cpp/siddon/siddon_gpu.cc:14-16),
+ * passed by value on the host instead of as device tensors that the
+ * reference reads back with blocking copies (siddon.cu.cc:403-405). */
+typedef struct nefct_grid {
+    int32_t nx, ny, nz;
+    float cx, cy, cz;
+    float sx, sy, sz;
+} nefct_grid;
+
+#define NEFCT_DET_FLAT 0
+#define NEFCT_DET_CYL  1
+
+/* Circular cone-beam geometry, reference kernel convention
+ * (nefct/cc/siddon_3d/siddon.cu.cc:341-353): at view angle phi the source
+ * sits at (-src_iso cos phi, -src_iso sin phi, z_off) and detector cell
+ * (ia, ib) at the rotation by phi of
+ *   flat: (src_det - src_iso, a, b)
+ *   cyl:  (src_det cos a - src_iso, src_det sin a, b)
+ * with a = (ia + a_shift) da - na da / 2,  b = (ib + b_shift) db - nb db / 2
+ * (+ z_off).  src_iso is the kernel's `SID`, src_det its `SAD` (the python
+ * geometry names them the other way round, quirk Q12).  a_shift/b_shift are
+ * the kernel's `ai`/`bi` (0.5 puts the cell centres symmetric about 0). */
+typedef struct nefct_cb_geom {
+    nefct_grid grid;
+    int32_t nv;                /* views */
+    const float *angles;       /* host, nv radians */
+    const float *z_offsets;    /* host, nv, or NULL for none */
+    float src_iso;             /* source -> rotation axis */
+    float src_det;             /* source -> detector */
+    int32_t na; float da; float a_shift;
+    int32_t nb; float db; float b_shift;
+    int32_t det_kind;          /* NEFCT_DET_FLAT / NEFCT_DET_CYL */
+} nefct_cb_geom;
+
+/* Walk switches.  With flags == 0 the forward reproduces siddon_3d's
+ * project_device (siddon.cu.cc:12-321): x drives when |xd| >= |yd| and each
+ * weight carries dx/L^2 (L = source-detector length in voxel units). */
+#define NEFCT_TIE_GT        0x01u /* x drives only when |xd| > |yd| (backproject_device :480, cpp/siddon :42) */
+#define NEFCT_SKIP_SHORT    0x02u /* skip rays with hypot(xd, yd) < 10 voxels (Q4: :472, cpp :33,:358) */
+#define NEFCT_NO_INV_L2     0x04u /* weights without 1/L^2: plain line integrals (backproject_device :526) */
+#define NEFCT_Q5            0x08u /* extra 1/L on y-driven three-voxel middle weights (cpp/siddon :292,:313) */
+#define NEFCT_Q8_INDEX      0x10u /* cylindrical backprojection reads the sinogram at ia + iv*na + ib*na*nb (:830) */
+#define NEFCT_NO_TRANSPOSE  0x20u /* x-driven rays read the x-fastest volume directly: no workspace, slower */
+
+/* presets */
+#define NEFCT_REF_FORWARD        0u                                              /* siddon_3d project_device */
+#define NEFCT_REF_BACKPROJECT    (NEFCT_TIE_GT | NEFCT_SKIP_SHORT | NEFCT_NO_INV_L2) /* siddon_3d backproject_device */
+#define NEFCT_LINE_INTEGRAL      NEFCT_NO_INV_L2
+#define NEFCT_LOR_REF_FORWARD    (NEFCT_TIE_GT | NEFCT_SKIP_SHORT | NEFCT_Q5)    /* cpp/siddon project_device */
+#define NEFCT_LOR_REF_BACKPROJECT (NEFCT_TIE_GT | NEFCT_SKIP_SHORT | NEFCT_NO_INV_L2)
+
+/* Bytes of workspace nefct_cb_forward / nefct_cb_backward need for this
+ * geometry and flags (a y-fastest copy of the volume; 0 with
+ * NEFCT_NO_TRANSPOSE).  Host-only, no CUDA call. */
+size_t nefct_cb_workspace_bytes(const nefct_cb_geom *g, uint32_t flags);
+
+/* Cone-beam forward projection vol -> sino.  Replaces ProjectFlat /
+ * ProjectCyli (nefct/cc/siddon_3d/siddon.cc:11-42, 114-224) and their host
+ * entry points project_flat / project_cyli (siddon.cu.cc:392-448).  The
+ * reference op passes da where db belongs (Q7, siddon.cc:155,211); callers
+ * that want that pass db = da. */
+nefct_status nefct_cb_forward(const nefct_cb_geom *g, const float *vol, float *sino, uint32_t flags,
+                              void *workspace, size_t workspace_bytes, void *stream);
+
+/* Cone-beam backprojection sino -> vol (vol is overwritten).  With the same
+ * flags as a forward call it is that forward's exact transpose; with
+ * NEFCT_REF_BACKPROJECT it reproduces BackProjectFlat / BackProjectCyli
+ * (siddon.cc:44-80, 226-348; siddon.cu.cc:450-890). */
+nefct_status nefct_cb_backward(const nefct_cb_geom *g, const float *sino, float *vol, uint32_t flags,
+                               void *workspace, size_t workspace_bytes, void *stream);
+
+/* FP64 builds of the same two operators (finite-difference and adjoint
+ * checks); geometry fields stay float. */
+nefct_status nefct_cb_forward_f64(const nefct_cb_geom *g, const double *vol, double *sino, uint32_t flags,
+                                  void *workspace, size_t workspace_bytes, void *stream);
+nefct_status nefct_cb_backward_f64(const nefct_cb_geom *g, const double *sino, double *vol, uint32_t flags,
+                                   void *workspace, size_t workspace_bytes, void *stream);
+
+/* Number of ray-voxel contributions (intersections) the forward with these
+ * flags makes, added into *count (device uint64).  No counterpart in the
+ * reference; it defines the throughput metric. */
+nefct_status nefct_cb_count_intersections(const nefct_cb_geom *g, uint32_t flags,
+                                          unsigned long long *count, void *stream);
+
+/* LOR projector pair.  lors is [6][n] (rows x1 y1 z1 x2 y2 z2, each n
+ * long), as the reference op slices it (cpp/siddon/siddon_gpu.cc:74-86).
+ * Replace Projection / Backprojection (siddon_gpu.cc:11-35) and their host
+ * entry points projection / backprojection (siddon_gpu.cu.cc:700-747).
+ * nefct_lor_forward writes every out[i] (0 for rays the reference skips
+ * without writing, Q4); nefct_lor_backward overwrites vol (the reference op
+ * accumulates into an unzeroed buffer, Q6). */
+nefct_status nefct_lor_forward(const nefct_grid *grid, const float *lors, int64_t n, const float *vol,
+                               float *out, uint32_t flags, void *stream);
+nefct_status nefct_lor_backward(const nefct_grid *grid, const float *lors, int64_t n, const float *vals,
+                                float *vol, uint32_t flags, void *stream);
+
+/* FDK.  Filter windows of mat_codes/filtering.m:63-88. */
+#define NEFCT_WIN_RAM_LAK     0
+#define NEFCT_WIN_SHEPP_LOGAN 1
+#define NEFCT_WIN_COSINE      2
+#define NEFCT_WIN_HAMMING     3
+#define NEFCT_WIN_HANN        4
+
+/* Cosine weight, optional Parker short-scan weight and ramp filtering of a
+ * flat-detector sinogram [nv][nb][na] -> out (same shape; may not alias).
+ * Follows mat_codes/filtering.m:5-48 and ParkerWeight.m:5-27 with DSD =
+ * src_det, DSO = src_iso, du = da, dv = db, u along detector columns.
+ * parker: 0 off, +1 / -1 on with ParkerWeight's `dir` = +1 / -1 (the view
+ * step is taken from angles[1] - angles[0]).  The zero-padded FFT
+ * convolution of the MATLAB code is evaluated as the equal direct linear
+ * convolution with the real, even spatial kernel. */
+nefct_status nefct_fdk_filter(const nefct_cb_geom *g, const float *sino, float *out, int32_t window,
+                              int32_t parker, void *stream);
+
+/* Voxel-driven bilinear backprojection filtered sino -> vol (overwritten):
+ * the geometry and index semantics of nefct/cc/pixel_3d/pixel.cu.cc:12-146
+ * (Q9-Q11; the grid is given by its centre here, the reference takes its
+ * low corner, Q10) times the FDK weight (src_iso / (src_iso + x'))^2 of
+ * mat_codes/backprojection.m:12.  NEFCT_FDK_NO_WEIGHT drops the weight,
+ * reproducing BackProjectFlat/BackProjectCyli of pixel_3d/pixel.cc:11-47. */
+#define NEFCT_FDK_NO_WEIGHT 0x100u
+nefct_status nefct_fdk_backproject(const nefct_cb_geom *g, const float *filtered, float *vol, uint32_t flags,
+                                   void *stream);
+
+/* Trilinear warp of cpp/deform (DeformKernel deform.cu.cc:13-46, op Deform
+ * deform.cc:12-22): out[i] = trilinear(img, i + m[i]), displacements in
+ * voxels, 0 where the reference returns early (base index <= 0 or the
+ * upper tap out of range, Q13).  All arrays [nz][ny][nx]. */
+nefct_status nefct_warp_forward(const float *img, const float *mx, const float *my, const float *mz,
+                                int32_t nx, int32_t ny, int32_t nz, float *out, void *stream);
+/* Adjoint of nefct_warp_forward with respect to img: gimg (overwritten) =
+ * W^T gout.  No counterpart in the reference (it has no gradients). */
+nefct_status nefct_warp_adjoint(const float *gout, const float *mx, const float *my, const float *mz,
+                                int32_t nx, int32_t ny, int32_t nz, float *gimg, void *stream);
+/* Gradient of <gout, warp(img, m)> with respect to the displacement field:
+ * gm* (overwritten).  No counterpart in the reference. */
+nefct_status nefct_warp_grad_dvf(const float *img, const float *mx, const float *my, const float *mz,
+                                 const float *gout, int32_t nx, int32_t ny, int32_t nz,
+                                 float *gmx, float *gmy, float *gmz, void *stream);
+nefct_status nefct_warp_forward_f64(const double *img, const double *mx, const double *my, const double *mz,
+                                    int32_t nx, int32_t ny, int32_t nz, double *out, void *stream);
+nefct_status nefct_warp_adjoint_f64(const double *gout, const double *mx, const double *my, const double *mz,
+                                    int32_t nx, int32_t ny, int32_t nz, double *gimg, void *stream);
+nefct_status nefct_warp_grad_dvf_f64(const double *img, const double *mx, const double *my, const double *mz,
+                                     const double *gout, int32_t nx, int32_t ny, int32_t nz,
+                                     double *gmx, double *gmy, double *gmz, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NEFCT_B200_H */

@@ -1,0 +1,123 @@
+"""Op-level mirrors of the reference's TensorFlow custom ops on this path.
+
+Same op names (TensorFlow's snake_case python wrappers), same inputs, attrs
+and output shapes as the registered ops, including their quirks:
+
+* ``siddon_3d``  nefct/cc/siddon_3d/siddon.cc:11-80 -- ProjectFlat,
+  ProjectCyli (the op passes ``da`` as the row pitch, Q7), BackProjectFlat,
+  BackProjectCyli (sinogram read transposed, Q8);
+* ``pixel_3d``   nefct/cc/pixel_3d/pixel.cc:11-47 -- voxel-driven
+  BackProjectFlat / BackProjectCyli (``center`` is the grid's low corner,
+  Q10; ``ai`` counts from the pixel centre, Q9);
+* ``siddon``     cpp/siddon/siddon_gpu.cc:11-35 -- Projection,
+  Backprojection (LOR pair);
+* ``deform``     cpp/deform/deform.cc:12-22 -- Deform.
+
+Tensors are CUDA torch tensors.  ``grid``/``center``/``size`` may be
+sequences or tensors; the reference reads them back from the device with
+blocking copies, here they are plain host values.  Backprojection outputs
+have the op's declared shape (nx, ny, nz) over the kernel's x-fastest memory,
+exactly like the TensorFlow tensors (reshape to (nz, ny, nx) for a
+[z][y][x] view).
+"""
+from __future__ import annotations
+
+import types
+
+import numpy as np
+import torch
+
+from . import _lib, ops
+
+__all__ = ["siddon_3d", "pixel_3d", "siddon", "deform"]
+
+
+def _host3(v, cast):
+    if isinstance(v, torch.Tensor):
+        v = v.detach().cpu().numpy()
+    v = np.asarray(v).reshape(-1)
+    if v.size != 3:
+        raise _lib.NefctError(_lib.ERR_INVALID, "grid/center/size need 3 entries")
+    return tuple(cast(x) for x in v)
+
+
+def _angles(angle):
+    if isinstance(angle, torch.Tensor):
+        angle = angle.detach().cpu().numpy()
+    return np.asarray(angle, np.float32).reshape(-1)
+
+
+def _geom(grid, center, size, angle, SID, SAD, na, da, ai, nb, db, bi, cyl):
+    g = _host3(grid, int)
+    return ops.ConeBeam(g, _angles(angle), float(SID), float(SAD), int(na), float(da), int(nb), float(db),
+                        float(ai), float(bi), _host3(center, float), _host3(size, float),
+                        "cyl" if cyl else "flat")
+
+
+def _flat_volume(image, g):
+    nx, ny, nz = g
+    if image.numel() != nx * ny * nz:
+        raise _lib.NefctError(_lib.ERR_INVALID, f"image has {image.numel()} elements, grid needs {nx * ny * nz}")
+    return image.contiguous().view(nz, ny, nx)
+
+
+def _project(cyl):
+    def op(image, grid, center, size, angle, SID, SAD, na, da, ai, nb, db, bi):
+        # Q7: the op hands da to the kernel where db belongs (siddon.cc:155, 211)
+        geom = _geom(grid, center, size, angle, SID, SAD, na, da, ai, nb, da, bi, cyl)
+        return ops.cb_forward(_flat_volume(image, geom.shape), geom, _lib.REF_FORWARD)
+    op.__name__ = "project_cyli" if cyl else "project_flat"
+    return op
+
+
+def _backproject(cyl):
+    def op(projection_value, grid, center, size, angle, SID, SAD, na, da, ai, nb, db, bi, nx, ny, nz):
+        geom = _geom(grid, center, size, angle, SID, SAD, na, da, ai, nb, db, bi, cyl)
+        flags = _lib.REF_BACKPROJECT | (_lib.Q8_INDEX if cyl else 0)
+        sino = projection_value.contiguous().view(geom.sino_shape)
+        vol = ops.cb_backward(sino, geom, flags)
+        return vol.view(int(nx), int(ny), int(nz))
+    op.__name__ = "back_project_cyli" if cyl else "back_project_flat"
+    return op
+
+
+def _pixel_backproject(cyl):
+    def op(projection_value, grid, center, size, angle, SID, SAD, na, da, ai, nb, db, bi, nx, ny, nz):
+        corner = _host3(center, float)
+        sz = _host3(size, float)
+        mid = tuple(c + s / 2.0 for c, s in zip(corner, sz))
+        # pixel_3d's ai/bi count from the pixel centre: siddon_3d's shift minus 1/2 (Q9)
+        geom = _geom(grid, mid, sz, angle, SID, SAD, na, da, float(ai) + 0.5, nb, db, float(bi) + 0.5, cyl)
+        sino = projection_value.contiguous().view(geom.sino_shape)
+        vol = ops.fdk_backproject(sino, geom, weight=False)
+        return vol.view(int(nx), int(ny), int(nz))
+    op.__name__ = "back_project_cyli" if cyl else "back_project_flat"
+    return op
+
+
+def _projection(lors, image, grid, center, size):
+    g = _host3(grid, int)
+    return ops.lor_forward(lors.contiguous(), _flat_volume(image, g), g, _host3(center, float),
+                           _host3(size, float), _lib.LOR_REF_FORWARD)
+
+
+def _backprojection(image, lors, lors_value, grid, center, size):
+    g = _host3(grid, int)
+    vol = ops.lor_backward(lors.contiguous(), lors_value.contiguous(), g, _host3(center, float),
+                           _host3(size, float), _lib.LOR_REF_BACKPROJECT)
+    return vol.view(image.shape)
+
+
+def _deform(image, mx, my, mz, grid):
+    g = _host3(grid, int)
+    vol = _flat_volume(image, g)
+    out = ops.warp_forward(vol, *[_flat_volume(m, g) for m in (mx, my, mz)])
+    return out.view(image.shape)
+
+
+siddon_3d = types.SimpleNamespace(project_flat=_project(False), project_cyli=_project(True),
+                                  back_project_flat=_backproject(False), back_project_cyli=_backproject(True))
+pixel_3d = types.SimpleNamespace(back_project_flat=_pixel_backproject(False),
+                                 back_project_cyli=_pixel_backproject(True))
+siddon = types.SimpleNamespace(projection=_projection, backprojection=_backprojection)
+deform = types.SimpleNamespace(deform=_deform)

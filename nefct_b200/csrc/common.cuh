@@ -1,0 +1,60 @@
+// Shared definitions of the nefct_b200 CUDA library (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <math.h>
+
+#include "nefct_b200.h"
+
+namespace nefct {
+
+// Records a message for nefct_last_error() and returns the status.
+nefct_status fail(nefct_status st, const char *fmt, ...);
+// Maps a CUDA error to NEFCT_ERR_CUDA with the call site in the message.
+nefct_status cuda_fail(cudaError_t e, const char *what);
+
+#define NEFCT_CHECK_CUDA(call)                                   \
+    do {                                                         \
+        cudaError_t e_ = (call);                                 \
+        if (e_ != cudaSuccess) return ::nefct::cuda_fail(e_, #call); \
+    } while (0)
+
+#define NEFCT_CHECK_LAUNCH(name)                                 \
+    do {                                                         \
+        cudaError_t e_ = cudaGetLastError();                     \
+        if (e_ != cudaSuccess) return ::nefct::cuda_fail(e_, name); \
+    } while (0)
+
+// Arithmetic with explicit round-to-nearest so the compiler cannot contract
+// a*b+c into one fused operation where the reference's evaluation order has
+// two roundings.  Used for every quantity that feeds a floor() or a branch.
+template <typename T> struct FP;
+template <> struct FP<float> {
+    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+    static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+    static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+    static __device__ __forceinline__ float sqrt(float a) { return __fsqrt_rn(a); }
+    static __device__ __forceinline__ int ifloor(float a) { return __float2int_rd(a); }
+};
+template <> struct FP<double> {
+    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+    static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+    static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+    static __device__ __forceinline__ double sqrt(double a) { return __dsqrt_rn(a); }
+    static __device__ __forceinline__ int ifloor(double a) { return __double2int_rd(a); }
+};
+
+// Views handled by one launch; the per-view table travels in the kernel's
+// parameter space (broadcast through the constant bank), so no device
+// buffer or host->device copy is needed for it.
+template <typename T> struct ViewTable {
+    static constexpr int kMax = sizeof(T) == 4 ? 1024 : 512;
+    T cs[kMax];
+    T sn[kMax];
+    T off[kMax];
+};
+
+}  // namespace nefct

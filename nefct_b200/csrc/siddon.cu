@@ -1,0 +1,495 @@
+// Cone-beam and LOR Siddon projectors on sm_100a, and their C-ABI entry
+// points (declared in include/nefct_b200.h).
+//
+// Launch shape: one thread per ray; a 256-thread CTA covers 32 adjacent
+// detector columns x 8 rows of one view, so each warp is 32 neighbouring
+// columns of one row.  Neighbouring rays of a warp cross a driving slab at
+// neighbouring transverse positions; with the transverse axis contiguous in
+// memory a warp's gather touches one or two 128-byte lines.  That holds for
+// y-driven rays in the x-fastest volume; x-driven rays read a y-fastest copy
+// of the volume (one transpose per call, in the caller's workspace).
+// Per-view cos/sin/z-offset ride in the kernel parameters.
+#include <math.h>
+#include <algorithm>
+
+#include "siddon.cuh"
+
+namespace nefct {
+
+template <typename T> struct CBParams {
+    GridDev<T> g;
+    int na, nb, nvc, v0, nv_total;
+    T src_iso, src_det, da, ai, db, bi, half_a, half_b;
+    int cyl;
+    uint32_t flags;
+    const T *vol;        // x-fastest volume (forward source)
+    const T *volT;       // y-fastest copy for x-driven rays, or nullptr
+    const T *sino;       // backward source, full sinogram
+    T *out;              // forward: full sinogram; backward: x-fastest volume
+    T *outT;             // backward: y-fastest accumulator, or nullptr
+    unsigned long long *count;
+    ViewTable<T> tab;
+};
+
+// Ray of detector cell (ia, ib) at view iv of the launch: ProjectFlatKernel
+// (siddon.cu.cc:341-353) / ProjectCyliKernel (:376-387), same order of
+// operations, plus the optional z offset of source and detector.
+template <typename T>
+__device__ __forceinline__ void cb_ray(const CBParams<T> &p, int ia, int ib, int iv, T *r)
+{
+    using F = FP<T>;
+    const T cs = p.tab.cs[iv], sn = p.tab.sn[iv], off = p.tab.off[iv];
+    const T a = F::sub(F::mul(F::add(p.ai, (T)ia), p.da), p.half_a);
+    const T b = F::sub(F::mul(F::add(p.bi, (T)ib), p.db), p.half_b);
+    T xd0, yd0;
+    if (p.cyl) {
+        xd0 = F::sub(F::mul(p.src_det, cos(a)), p.src_iso);
+        yd0 = F::mul(p.src_det, sin(a));
+    } else {
+        xd0 = F::sub(p.src_det, p.src_iso);
+        yd0 = a;
+    }
+    r[0] = F::mul(-p.src_iso, cs);
+    r[1] = F::mul(-p.src_iso, sn);
+    r[2] = F::add((T)0, off);
+    r[3] = F::sub(F::mul(xd0, cs), F::mul(yd0, sn));
+    r[4] = F::add(F::mul(xd0, sn), F::mul(yd0, cs));
+    r[5] = F::add(b, off);
+}
+
+template <typename T> struct GatherOp {
+    const T *__restrict__ base;
+    int su, sv, sw;
+    T acc;
+    __device__ __forceinline__ void operator()(int k, int cv, int cw, T r, T W)
+    {
+        acc += __ldg(base + (k * su + cv * sv + cw * sw)) * (r * W);
+    }
+};
+
+template <typename T> struct ScatterOp {
+    T *base;
+    int su, sv, sw;
+    T y;
+    __device__ __forceinline__ void operator()(int k, int cv, int cw, T r, T W)
+    {
+        atomicAdd(base + (k * su + cv * sv + cw * sw), y * (r * W));
+    }
+};
+
+struct CountOp {
+    unsigned n;
+    template <typename T> __device__ __forceinline__ void operator()(int, int, int, T, T) { ++n; }
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) cb_forward_kernel(const __grid_constant__ CBParams<T> p)
+{
+    const int ia = blockIdx.x * 32 + threadIdx.x;
+    const int ib = blockIdx.y * 8 + threadIdx.y;
+    const int iv = blockIdx.z;
+    if (ia >= p.na || ib >= p.nb) return;
+    T r[6];
+    cb_ray(p, ia, ib, iv, r);
+    Walk<T> w;
+    T acc = (T)0;
+    if (setup_walk(p.g, r, p.flags, w)) {
+        GatherOp<T> op;
+        op.sw = p.g.nx * p.g.ny;
+        if (!w.xdrive) { op.base = p.vol; op.su = p.g.nx; op.sv = 1; }
+        else if (p.volT) { op.base = p.volT; op.su = p.g.ny; op.sv = 1; }
+        else { op.base = p.vol; op.su = 1; op.sv = p.g.nx; }
+        op.acc = (T)0;
+        run_walk(w, p.g, op);
+        acc = op.acc;
+    }
+    p.out[(size_t)(p.v0 + iv) * p.na * p.nb + (size_t)ib * p.na + ia] = acc;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) cb_backward_kernel(const __grid_constant__ CBParams<T> p)
+{
+    const int ia = blockIdx.x * 32 + threadIdx.x;
+    const int ib = blockIdx.y * 8 + threadIdx.y;
+    const int iv = blockIdx.z;
+    if (ia >= p.na || ib >= p.nb) return;
+    const size_t total = (size_t)p.na * p.nb * p.nv_total;
+    const size_t vg = (size_t)(p.v0 + iv);
+    // Q8: the reference's cylindrical backprojection reads ia + iv*na + ib*na*nb
+    const size_t id = (p.flags & NEFCT_Q8_INDEX) ? (size_t)ia + vg * p.na + (size_t)ib * p.na * p.nb
+                                                 : vg * p.na * p.nb + (size_t)ib * p.na + ia;
+    const T y = id < total ? p.sino[id] : (T)0;
+    if (y == (T)0) return;
+    T r[6];
+    cb_ray(p, ia, ib, iv, r);
+    Walk<T> w;
+    if (!setup_walk(p.g, r, p.flags, w)) return;
+    ScatterOp<T> op;
+    op.sw = p.g.nx * p.g.ny;
+    op.y = y;
+    if (!w.xdrive) { op.base = p.out; op.su = p.g.nx; op.sv = 1; }
+    else if (p.outT) { op.base = p.outT; op.su = p.g.ny; op.sv = 1; }
+    else { op.base = p.out; op.su = 1; op.sv = p.g.nx; }
+    run_walk(w, p.g, op);
+}
+
+__global__ void __launch_bounds__(256) cb_count_kernel(const __grid_constant__ CBParams<float> p)
+{
+    const int ia = blockIdx.x * 32 + threadIdx.x;
+    const int ib = blockIdx.y * 8 + threadIdx.y;
+    const int iv = blockIdx.z;
+    unsigned n = 0;
+    if (ia < p.na && ib < p.nb) {
+        float r[6];
+        cb_ray(p, ia, ib, iv, r);
+        Walk<float> w;
+        if (setup_walk(p.g, r, p.flags, w)) {
+            CountOp op{0};
+            run_walk(w, p.g, op);
+            n = op.n;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+    if ((threadIdx.x & 31) == 0 && n) atomicAdd(p.count, (unsigned long long)n);
+}
+
+// out[z][x][y] = in[z][y][x] (32x32 tiles through shared memory)
+template <typename T>
+__global__ void __launch_bounds__(256) transpose_xy_kernel(const T *__restrict__ in, T *__restrict__ out,
+                                                           int nx, int ny)
+{
+    __shared__ T tile[32][33];
+    const size_t plane = (size_t)nx * ny * blockIdx.z;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int x = x0 + threadIdx.x, y = y0 + j;
+        if (x < nx && y < ny) tile[j][threadIdx.x] = in[plane + (size_t)y * nx + x];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int y = y0 + threadIdx.x, x = x0 + j;
+        if (x < nx && y < ny) out[plane + (size_t)x * ny + y] = tile[threadIdx.x][j];
+    }
+}
+
+// vol[z][y][x] += accT[z][x][y]
+template <typename T>
+__global__ void __launch_bounds__(256) fold_add_kernel(const T *__restrict__ accT, T *__restrict__ vol,
+                                                       int nx, int ny)
+{
+    __shared__ T tile[32][33];
+    const size_t plane = (size_t)nx * ny * blockIdx.z;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int y = y0 + threadIdx.x, x = x0 + j;
+        if (x < nx && y < ny) tile[j][threadIdx.x] = accT[plane + (size_t)x * ny + y];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int x = x0 + threadIdx.x, y = y0 + j;
+        if (x < nx && y < ny) vol[plane + (size_t)y * nx + x] += tile[threadIdx.x][j];
+    }
+}
+
+// ---------------- LOR projector pair (cpp/siddon) ----------------
+
+template <typename T> struct LorParams {
+    GridDev<T> g;
+    const T *lors;
+    long long n;
+    uint32_t flags;
+    const T *vol;
+    const T *vals;
+    T *out;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) lor_forward_kernel(const __grid_constant__ LorParams<T> p)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < p.n;
+         i += (long long)gridDim.x * blockDim.x) {
+        T r[6];
+        for (int j = 0; j < 6; ++j) r[j] = p.lors[j * p.n + i];
+        Walk<T> w;
+        T acc = (T)0;
+        if (setup_walk(p.g, r, p.flags, w)) {
+            GatherOp<T> op;
+            op.base = p.vol; op.sw = p.g.nx * p.g.ny; op.acc = (T)0;
+            if (w.xdrive) { op.su = 1; op.sv = p.g.nx; } else { op.su = p.g.nx; op.sv = 1; }
+            run_walk(w, p.g, op);
+            acc = op.acc;
+        }
+        p.out[i] = acc;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) lor_backward_kernel(const __grid_constant__ LorParams<T> p)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < p.n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const T y = p.vals[i];
+        if (y == (T)0) continue;
+        T r[6];
+        for (int j = 0; j < 6; ++j) r[j] = p.lors[j * p.n + i];
+        Walk<T> w;
+        if (!setup_walk(p.g, r, p.flags, w)) continue;
+        ScatterOp<T> op;
+        op.base = p.out; op.sw = p.g.nx * p.g.ny; op.y = y;
+        if (w.xdrive) { op.su = 1; op.sv = p.g.nx; } else { op.su = p.g.nx; op.sv = 1; }
+        run_walk(w, p.g, op);
+    }
+}
+
+// ---------------- host side ----------------
+
+static const uint32_t kWalkFlags = NEFCT_TIE_GT | NEFCT_SKIP_SHORT | NEFCT_NO_INV_L2 | NEFCT_Q5 |
+                                   NEFCT_Q8_INDEX | NEFCT_NO_TRANSPOSE;
+
+static nefct_status check_grid(const nefct_grid &g)
+{
+    if (g.nx < 1 || g.ny < 1 || g.nz < 1)
+        return fail(NEFCT_ERR_INVALID, "grid dimensions must be >= 1 (got %d x %d x %d)", g.nx, g.ny, g.nz);
+    if ((long long)g.nx * g.ny * g.nz >= (1ll << 31))
+        return fail(NEFCT_ERR_INVALID, "grid has %lld voxels; at most 2^31-1 are supported",
+                    (long long)g.nx * g.ny * g.nz);
+    const float v[6] = {g.cx, g.cy, g.cz, g.sx, g.sy, g.sz};
+    for (int i = 0; i < 6; ++i)
+        if (!std::isfinite(v[i])) return fail(NEFCT_ERR_INVALID, "grid centre/size must be finite");
+    if (!(g.sx > 0.f && g.sy > 0.f && g.sz > 0.f)) return fail(NEFCT_ERR_INVALID, "grid size must be > 0");
+    return NEFCT_OK;
+}
+
+nefct_status check_cb_geom(const nefct_cb_geom *g)
+{
+    if (!g) return fail(NEFCT_ERR_INVALID, "geometry is NULL");
+    nefct_status st = check_grid(g->grid);
+    if (st) return st;
+    if (g->nv < 1 || !g->angles) return fail(NEFCT_ERR_INVALID, "need nv >= 1 view angles (nv=%d)", g->nv);
+    if (g->na < 1 || g->nb < 1) return fail(NEFCT_ERR_INVALID, "detector must be >= 1 x 1 (got %d x %d)", g->na, g->nb);
+    if ((long long)g->na * g->nb * g->nv >= (1ll << 40))
+        return fail(NEFCT_ERR_INVALID, "sinogram too large");
+    if ((long long)g->na * g->nb >= (1ll << 31)) return fail(NEFCT_ERR_INVALID, "detector too large");
+    if (g->det_kind != NEFCT_DET_FLAT && g->det_kind != NEFCT_DET_CYL)
+        return fail(NEFCT_ERR_INVALID, "det_kind must be NEFCT_DET_FLAT or NEFCT_DET_CYL (got %d)", g->det_kind);
+    const float v[6] = {g->src_iso, g->src_det, g->da, g->a_shift, g->db, g->b_shift};
+    for (int i = 0; i < 6; ++i)
+        if (!std::isfinite(v[i])) return fail(NEFCT_ERR_INVALID, "scanner geometry must be finite");
+    if (g->da == 0.f || g->db == 0.f) return fail(NEFCT_ERR_INVALID, "detector pitch must be non-zero");
+    for (int i = 0; i < g->nv; ++i) {
+        if (!std::isfinite(g->angles[i])) return fail(NEFCT_ERR_INVALID, "angle %d is not finite", i);
+        if (g->z_offsets && !std::isfinite(g->z_offsets[i]))
+            return fail(NEFCT_ERR_INVALID, "z offset %d is not finite", i);
+    }
+    return NEFCT_OK;
+}
+
+template <typename T> static void fill_cb_params(CBParams<T> &p, const nefct_cb_geom *g, uint32_t flags)
+{
+    p.g = make_grid_dev<T>(g->grid);
+    p.na = g->na; p.nb = g->nb; p.nv_total = g->nv;
+    p.src_iso = (T)g->src_iso; p.src_det = (T)g->src_det;
+    p.da = (T)g->da; p.ai = (T)g->a_shift; p.db = (T)g->db; p.bi = (T)g->b_shift;
+    // na*da/2 in the reference's order (siddon.cu.cc:341)
+    p.half_a = (T)g->na * p.da / (T)2;
+    p.half_b = (T)g->nb * p.db / (T)2;
+    p.cyl = g->det_kind == NEFCT_DET_CYL;
+    p.flags = flags;
+}
+
+// cos/sin of the view angles from the double-precision functions, rounded.
+template <typename T> static void fill_views(CBParams<T> &p, const nefct_cb_geom *g, int v0, int nvc)
+{
+    p.v0 = v0; p.nvc = nvc;
+    for (int i = 0; i < nvc; ++i) {
+        const double a = (double)g->angles[v0 + i];
+        p.tab.cs[i] = (T)cos(a);
+        p.tab.sn[i] = (T)sin(a);
+        p.tab.off[i] = g->z_offsets ? (T)g->z_offsets[v0 + i] : (T)0;
+    }
+}
+
+template <typename T>
+static nefct_status transpose_xy(const T *in, T *out, const nefct_grid &g, cudaStream_t s)
+{
+    dim3 grid((g.nx + 31) / 32, (g.ny + 31) / 32, g.nz);
+    transpose_xy_kernel<T><<<grid, dim3(32, 8), 0, s>>>(in, out, g.nx, g.ny);
+    NEFCT_CHECK_LAUNCH("transpose_xy_kernel");
+    return NEFCT_OK;
+}
+
+template <typename T>
+static nefct_status cb_forward_impl(const nefct_cb_geom *g, const T *vol, T *sino, uint32_t flags, void *ws,
+                                    size_t wsb, cudaStream_t s)
+{
+    nefct_status st = check_cb_geom(g);
+    if (st) return st;
+    if (!vol || !sino) return fail(NEFCT_ERR_INVALID, "vol and sino must be non-NULL");
+    if (flags & ~kWalkFlags) return fail(NEFCT_ERR_INVALID, "unknown flag bits 0x%x", flags & ~kWalkFlags);
+    CBParams<T> *p = new CBParams<T>();
+    fill_cb_params(*p, g, flags);
+    p->vol = vol;
+    p->out = sino;
+    const size_t nvox = (size_t)g->grid.nx * g->grid.ny * g->grid.nz;
+    if (!(flags & NEFCT_NO_TRANSPOSE)) {
+        if (!ws || wsb < nvox * sizeof(T)) {
+            delete p;
+            return fail(NEFCT_ERR_WORKSPACE, "forward needs %zu workspace bytes, got %zu", nvox * sizeof(T), wsb);
+        }
+        st = transpose_xy(vol, (T *)ws, g->grid, s);
+        if (st) { delete p; return st; }
+        p->volT = (const T *)ws;
+    }
+    const int kMax = ViewTable<T>::kMax;
+    for (int v0 = 0; v0 < g->nv; v0 += kMax) {
+        const int nvc = std::min(kMax, g->nv - v0);
+        fill_views(*p, g, v0, nvc);
+        dim3 grid((g->na + 31) / 32, (g->nb + 7) / 8, nvc);
+        cb_forward_kernel<T><<<grid, dim3(32, 8), 0, s>>>(*p);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) { delete p; return cuda_fail(e, "cb_forward_kernel"); }
+    }
+    delete p;
+    return NEFCT_OK;
+}
+
+template <typename T>
+static nefct_status cb_backward_impl(const nefct_cb_geom *g, const T *sino, T *vol, uint32_t flags, void *ws,
+                                     size_t wsb, cudaStream_t s)
+{
+    nefct_status st = check_cb_geom(g);
+    if (st) return st;
+    if (!vol || !sino) return fail(NEFCT_ERR_INVALID, "vol and sino must be non-NULL");
+    if (flags & ~kWalkFlags) return fail(NEFCT_ERR_INVALID, "unknown flag bits 0x%x", flags & ~kWalkFlags);
+    const size_t nvox = (size_t)g->grid.nx * g->grid.ny * g->grid.nz;
+    const bool tr = !(flags & NEFCT_NO_TRANSPOSE);
+    if (tr && (!ws || wsb < nvox * sizeof(T)))
+        return fail(NEFCT_ERR_WORKSPACE, "backward needs %zu workspace bytes, got %zu", nvox * sizeof(T), wsb);
+    CBParams<T> *p = new CBParams<T>();
+    fill_cb_params(*p, g, flags);
+    p->sino = sino;
+    p->out = vol;
+    p->outT = tr ? (T *)ws : nullptr;
+    cudaError_t e = cudaMemsetAsync(vol, 0, nvox * sizeof(T), s);
+    if (e == cudaSuccess && tr) e = cudaMemsetAsync(ws, 0, nvox * sizeof(T), s);
+    if (e != cudaSuccess) { delete p; return cuda_fail(e, "cudaMemsetAsync"); }
+    const int kMax = ViewTable<T>::kMax;
+    for (int v0 = 0; v0 < g->nv; v0 += kMax) {
+        const int nvc = std::min(kMax, g->nv - v0);
+        fill_views(*p, g, v0, nvc);
+        dim3 grid((g->na + 31) / 32, (g->nb + 7) / 8, nvc);
+        cb_backward_kernel<T><<<grid, dim3(32, 8), 0, s>>>(*p);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) { delete p; return cuda_fail(e, "cb_backward_kernel"); }
+    }
+    delete p;
+    if (tr) {
+        dim3 grid((g->grid.nx + 31) / 32, (g->grid.ny + 31) / 32, g->grid.nz);
+        fold_add_kernel<T><<<grid, dim3(32, 8), 0, s>>>((const T *)ws, vol, g->grid.nx, g->grid.ny);
+        NEFCT_CHECK_LAUNCH("fold_add_kernel");
+    }
+    return NEFCT_OK;
+}
+
+template <typename T>
+static nefct_status lor_impl(const nefct_grid *grid, const T *lors, int64_t n, const T *src, T *dst,
+                             uint32_t flags, cudaStream_t s, bool forward)
+{
+    if (!grid) return fail(NEFCT_ERR_INVALID, "grid is NULL");
+    nefct_status st = check_grid(*grid);
+    if (st) return st;
+    if (n < 0) return fail(NEFCT_ERR_INVALID, "negative LOR count");
+    if ((!lors || !src || !dst) && n > 0) return fail(NEFCT_ERR_INVALID, "NULL buffer");
+    if (flags & ~kWalkFlags) return fail(NEFCT_ERR_INVALID, "unknown flag bits 0x%x", flags & ~kWalkFlags);
+    if (!dst) return fail(NEFCT_ERR_INVALID, "NULL output");
+    LorParams<T> p;
+    p.g = make_grid_dev<T>(*grid);
+    p.lors = lors; p.n = n; p.flags = flags;
+    if (!forward) {
+        const size_t nvox = (size_t)grid->nx * grid->ny * grid->nz;
+        NEFCT_CHECK_CUDA(cudaMemsetAsync(dst, 0, nvox * sizeof(T), s));
+        p.vals = src; p.out = dst; p.vol = nullptr;
+    } else {
+        p.vol = src; p.out = dst; p.vals = nullptr;
+    }
+    if (n == 0) return NEFCT_OK;
+    const long long blocks = std::min<long long>((n + 255) / 256, 148ll * 64);
+    if (forward) lor_forward_kernel<T><<<(unsigned)blocks, 256, 0, s>>>(p);
+    else lor_backward_kernel<T><<<(unsigned)blocks, 256, 0, s>>>(p);
+    NEFCT_CHECK_LAUNCH(forward ? "lor_forward_kernel" : "lor_backward_kernel");
+    return NEFCT_OK;
+}
+
+}  // namespace nefct
+
+using namespace nefct;
+
+extern "C" {
+
+size_t nefct_cb_workspace_bytes(const nefct_cb_geom *g, uint32_t flags)
+{
+    if (!g || (flags & NEFCT_NO_TRANSPOSE)) return 0;
+    return (size_t)(g->grid.nx > 0 ? g->grid.nx : 0) * (size_t)(g->grid.ny > 0 ? g->grid.ny : 0) *
+           (size_t)(g->grid.nz > 0 ? g->grid.nz : 0) * sizeof(float);
+}
+
+nefct_status nefct_cb_forward(const nefct_cb_geom *g, const float *vol, float *sino, uint32_t flags,
+                              void *ws, size_t wsb, void *stream)
+{
+    return cb_forward_impl<float>(g, vol, sino, flags, ws, wsb, (cudaStream_t)stream);
+}
+
+nefct_status nefct_cb_backward(const nefct_cb_geom *g, const float *sino, float *vol, uint32_t flags,
+                               void *ws, size_t wsb, void *stream)
+{
+    return cb_backward_impl<float>(g, sino, vol, flags, ws, wsb, (cudaStream_t)stream);
+}
+
+nefct_status nefct_cb_forward_f64(const nefct_cb_geom *g, const double *vol, double *sino, uint32_t flags,
+                                  void *ws, size_t wsb, void *stream)
+{
+    return cb_forward_impl<double>(g, vol, sino, flags, ws, wsb, (cudaStream_t)stream);
+}
+
+nefct_status nefct_cb_backward_f64(const nefct_cb_geom *g, const double *sino, double *vol, uint32_t flags,
+                                   void *ws, size_t wsb, void *stream)
+{
+    return cb_backward_impl<double>(g, sino, vol, flags, ws, wsb, (cudaStream_t)stream);
+}
+
+nefct_status nefct_cb_count_intersections(const nefct_cb_geom *g, uint32_t flags, unsigned long long *count,
+                                          void *stream)
+{
+    nefct_status st = check_cb_geom(g);
+    if (st) return st;
+    if (!count) return fail(NEFCT_ERR_INVALID, "count is NULL");
+    if (flags & ~kWalkFlags) return fail(NEFCT_ERR_INVALID, "unknown flag bits 0x%x", flags & ~kWalkFlags);
+    CBParams<float> *p = new CBParams<float>();
+    fill_cb_params(*p, g, flags);
+    p->count = count;
+    const int kMax = ViewTable<float>::kMax;
+    for (int v0 = 0; v0 < g->nv; v0 += kMax) {
+        const int nvc = std::min(kMax, g->nv - v0);
+        fill_views(*p, g, v0, nvc);
+        dim3 grid((g->na + 31) / 32, (g->nb + 7) / 8, nvc);
+        cb_count_kernel<<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>(*p);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) { delete p; return cuda_fail(e, "cb_count_kernel"); }
+    }
+    delete p;
+    return NEFCT_OK;
+}
+
+nefct_status nefct_lor_forward(const nefct_grid *grid, const float *lors, int64_t n, const float *vol,
+                               float *out, uint32_t flags, void *stream)
+{
+    return lor_impl<float>(grid, lors, n, vol, out, flags, (cudaStream_t)stream, true);
+}
+
+nefct_status nefct_lor_backward(const nefct_grid *grid, const float *lors, int64_t n, const float *vals,
+                                float *vol, uint32_t flags, void *stream)
+{
+    return lor_impl<float>(grid, lors, n, vals, vol, flags, (cudaStream_t)stream, false);
+}
+
+}  // extern "C"

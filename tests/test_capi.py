@@ -1,0 +1,92 @@
+"""CPU: the C-ABI library loads, exports every symbol the header declares, and
+rejects bad arguments with a status (no GPU work is started by these calls:
+validation happens before any CUDA call)."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    hdr = open(os.path.join(ROOT, "include", "nefct_b200.h")).read()
+    hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
+    return sorted(set(re.findall(r"\b(nefct_[a-z0-9_]+)\s*\(", hdr)))
+
+
+def test_every_declared_symbol_is_exported(nefct_lib):
+    syms = declared_symbols()
+    assert len(syms) >= 19
+    for s in syms:
+        assert hasattr(nefct_lib, s), s
+
+
+def test_python_binding_covers_header(nefct_lib):
+    from nefct_b200 import _lib
+    assert sorted(_lib.symbols()) == declared_symbols()
+
+
+def test_version_and_status_strings(nefct_lib):
+    assert b"sm_100a" in nefct_lib.nefct_version()
+    assert nefct_lib.nefct_status_string(0) == b"ok"
+    assert nefct_lib.nefct_status_string(3).startswith(b"workspace")
+
+
+def _geom(**kw):
+    import nefct_b200 as nb
+    base = dict(shape=(16, 16, 16), angles=np.linspace(0, 6.28, 8, dtype=np.float32), src_iso=100.0,
+                src_det=200.0, na=32, da=1.0, nb=24, db=1.0)
+    base.update(kw)
+    return nb.ConeBeam(**base)
+
+
+@pytest.mark.parametrize("kw,needle", [
+    (dict(na=0), b"detector"),
+    (dict(shape=(0, 16, 16)), b"grid dimensions"),
+    (dict(da=0.0), b"pitch"),
+    (dict(angles=np.array([0.0, np.nan], np.float32)), b"angle 1"),
+    (dict(size=(16.0, -1.0, 16.0)), b"size"),
+])
+def test_invalid_geometry_is_rejected(nefct_lib, kw, needle):
+    g = _geom(**kw).struct()
+    st = nefct_lib.nefct_cb_forward(C.byref(g), None, None, 0, None, 0, None)
+    assert st == 1
+    assert needle in nefct_lib.nefct_last_error()
+
+
+def test_forward_needs_workspace(nefct_lib):
+    g = _geom().struct()
+    # non-NULL fake pointers: validation fails on the workspace before any CUDA call
+    st = nefct_lib.nefct_cb_forward(C.byref(g), C.c_void_p(16), C.c_void_p(16), 0, None, 0, None)
+    assert st == 3
+    assert nefct_lib.nefct_cb_workspace_bytes(C.byref(g), 0) == 16 ** 3 * 4
+    assert nefct_lib.nefct_cb_workspace_bytes(C.byref(g), 0x20) == 0
+
+
+def test_unknown_flags_rejected(nefct_lib):
+    g = _geom().struct()
+    st = nefct_lib.nefct_cb_forward(C.byref(g), C.c_void_p(16), C.c_void_p(16), 0x4000, None, 0, None)
+    assert st == 1 and b"flag" in nefct_lib.nefct_last_error()
+
+
+def test_fdk_rejects_cylindrical_and_bad_window(nefct_lib):
+    g = _geom(det_kind="cyl").struct()
+    assert nefct_lib.nefct_fdk_filter(C.byref(g), C.c_void_p(16), C.c_void_p(32), 0, 0, None) == 5
+    g = _geom().struct()
+    assert nefct_lib.nefct_fdk_filter(C.byref(g), C.c_void_p(16), C.c_void_p(32), 9, 0, None) == 1
+    assert nefct_lib.nefct_fdk_filter(C.byref(g), C.c_void_p(16), C.c_void_p(16), 0, 0, None) == 1
+
+
+def test_warp_rejects_bad_grid(nefct_lib):
+    assert nefct_lib.nefct_warp_forward(None, None, None, None, 0, 4, 4, None, None) == 1
+
+
+def test_ops_refuse_cpu_tensors(nefct_lib):
+    import torch
+    import nefct_b200 as nb
+    g = _geom()
+    with pytest.raises(nb.NefctError, match="CUDA tensor"):
+        nb.ops.cb_forward(torch.zeros(g.vol_shape), g)

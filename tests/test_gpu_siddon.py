@@ -1,0 +1,213 @@
+"""GPU parity of the Siddon kernels (called through the C ABI via ctypes).
+
+Tolerances (float32): rel-L2 <= 1e-5 and max-abs <= 1e-4 * max|ref| against
+the reference (golden fixtures / reference build / oracle restatement);
+FP64 identities to 1e-12.
+"""
+import numpy as np
+import pytest
+import torch
+
+import nefct_b200 as nb
+from nefct_b200 import _lib, ops
+from tests.golden.make_golden import AI, BI, CASES, DB, NA, NB, SRC_DET, SRC_ISO
+
+pytestmark = pytest.mark.gpu
+
+REL_L2 = 1e-5
+MAX_ABS = 1e-4
+
+
+def assert_parity(out, ref, rel=REL_L2, mabs=MAX_ABS):
+    out = np.asarray(out, np.float64)
+    ref = np.asarray(ref, np.float64)
+    scale = np.abs(ref).max()
+    assert scale > 0
+    r = np.linalg.norm(out - ref) / np.linalg.norm(ref)
+    m = np.abs(out - ref).max() / scale
+    assert r <= rel and m <= mabs, f"rel-L2 {r:.3e} max-abs/max {m:.3e}"
+    return r
+
+
+def _geom(case, angles):
+    name, grid, centre, size, cyl, da = case
+    return nb.ConeBeam(grid, angles, SRC_ISO, SRC_DET, NA, da, NB, DB, AI, BI, centre, size,
+                       "cyl" if cyl else "flat")
+
+
+@pytest.mark.parametrize("flags", [0, _lib.NO_TRANSPOSE], ids=["transposed", "direct"])
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_forward_vs_reference_fixtures(cuda, golden, case, flags):
+    g = _geom(case, golden["angles"])
+    vol = torch.from_numpy(golden[f"{case[0]}/vol"]).to(cuda)
+    out = ops.cb_forward(vol, g, flags).cpu().numpy()
+    assert_parity(out, golden[f"{case[0]}/fwd"])
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_forward_vs_restatement_tight(cuda, golden, oracle_lib, case):
+    """Same per-view trig as the GPU (double rounded): only weight rounding differs."""
+    name, grid, centre, size, cyl, da = case
+    g = _geom(case, golden["angles"])
+    vol = golden[f"{name}/vol"]
+    out = ops.cb_forward(torch.from_numpy(vol).to(cuda), g).cpu().numpy()
+    port, _ = oracle_lib.cb_forward(oracle_lib.grid(grid, centre, size), vol, golden["angles"], SRC_ISO,
+                                    SRC_DET, NA, da, AI, NB, DB, BI, cyl=cyl, use_cosf=False)
+    assert_parity(out, port, rel=1e-6, mabs=1e-5)
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_reference_backprojection_vs_fixtures(cuda, golden, case):
+    name, grid, centre, size, cyl, da = case
+    g = _geom(case, golden["angles"])
+    sino = torch.from_numpy(golden[f"{name}/sino_in"]).to(cuda)
+    flags = _lib.REF_BACKPROJECT | (_lib.Q8_INDEX if cyl else 0)
+    out = ops.cb_backward(sino, g, flags).cpu().numpy()
+    assert_parity(out, golden[f"{name}/bp"])
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_intersection_count_matches_reference(cuda, golden, case):
+    g = _geom(case, golden["angles"])
+    assert ops.cb_count_intersections(g) == int(golden[f"{case[0]}/count"])
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_exact_transpose_vs_oracle(cuda, golden, oracle_lib, case):
+    """cb_backward with the forward's flags equals the oracle's scatter with
+    the forward's weights (tie >=, 1/L^2, no skip)."""
+    name, grid, centre, size, cyl, da = case
+    g = _geom(case, golden["angles"])
+    sino = golden[f"{name}/sino_in"]
+    out = ops.cb_backward(torch.from_numpy(sino).to(cuda), g, 0).cpu().numpy()
+    ref = oracle_lib.cb_backward(oracle_lib.grid(grid, centre, size), sino, golden["angles"], SRC_ISO,
+                                 SRC_DET, NA, da, AI, NB, DB, BI, cyl=cyl, flags=oracle_lib.CB_FWD)
+    assert_parity(out, ref)
+
+
+@pytest.mark.parametrize("flags", [0, _lib.LINE_INTEGRAL, _lib.REF_BACKPROJECT])
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_adjoint_identity_f64(cuda, case, flags):
+    """<A x, y> == <x, A^T y> to rounding in FP64 for every flag set."""
+    g = _geom(case, np.linspace(0, 2 * np.pi, 17, endpoint=False) + 0.05)
+    gen = torch.Generator(device=cuda).manual_seed(34)
+    x = torch.randn(g.vol_shape, dtype=torch.float64, device=cuda, generator=gen)
+    y = torch.randn(g.sino_shape, dtype=torch.float64, device=cuda, generator=gen)
+    ax = ops.cb_forward(x, g, flags)
+    aty = ops.cb_backward(y, g, flags)
+    lhs, rhs = float((ax * y).sum()), float((x * aty).sum())
+    assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), 1.0) * 1e2
+
+
+def test_f64_forward_vs_reference_f64(cuda, golden):
+    for case in CASES:
+        g = _geom(case, golden["angles"])
+        vol = torch.from_numpy(golden[f"{case[0]}/vol"].astype(np.float64)).to(cuda)
+        out = ops.cb_forward(vol, g).cpu().numpy()
+        assert_parity(out, golden[f"{case[0]}/fwd64"], rel=1e-6, mabs=1e-6)
+
+
+def test_finite_difference_fp64_autograd(cuda):
+    """loss = ||A x - b||^2 on 32^3 / 60 views in FP64: autograd (hand-written
+    transpose) against central differences along a random direction."""
+    g = nb.ConeBeam((32, 32, 32), np.linspace(0, 2 * np.pi, 60, endpoint=False), 120.0, 240.0, 48, 1.5, 40, 1.5)
+    gen = torch.Generator(device=cuda).manual_seed(5)
+    x = torch.rand(g.vol_shape, dtype=torch.float64, device=cuda, generator=gen).requires_grad_()
+    b = torch.rand(g.sino_shape, dtype=torch.float64, device=cuda, generator=gen)
+    d = torch.randn(g.vol_shape, dtype=torch.float64, device=cuda, generator=gen)
+    loss = ((nb.project(x, g) - b) ** 2).sum()
+    loss.backward()
+    h = 1e-4
+    with torch.no_grad():
+        fp = ((ops.cb_forward(x + h * d, g) - b) ** 2).sum()
+        fm = ((ops.cb_forward(x - h * d, g) - b) ** 2).sum()
+    fd = float((fp - fm) / (2 * h))
+    an = float((x.grad * d).sum())
+    assert abs(fd - an) <= 1e-8 * abs(an)
+
+
+def test_many_views_chunked_and_offsets(cuda, oracle_lib):
+    """> 1024 views (several launches) and per-view z offsets."""
+    nv = 1100
+    ang = np.linspace(0, 2 * np.pi, nv, endpoint=False).astype(np.float32)
+    off = np.linspace(-3, 3, nv).astype(np.float32)
+    g = nb.ConeBeam((12, 12, 10), ang, 60.0, 120.0, 20, 1.5, 9, 1.5, z_offsets=off)
+    vol = np.random.default_rng(3).random((10, 12, 12), dtype=np.float32)
+    out = ops.cb_forward(torch.from_numpy(vol).to(cuda), g).cpu().numpy()
+    ref, _ = oracle_lib.cb_forward(oracle_lib.grid((12, 12, 10)), vol, ang, 60.0, 120.0, 20, 1.5, 0.5, 9, 1.5,
+                                   0.5, off=off)
+    assert_parity(out, ref)
+
+
+def test_config1_full_size_vs_reference(cuda, oracle_lib):
+    """Configuration 1 (64^3 at 2 mm, 10 seeded ellipsoids, 90 views, 128x96
+    at 2 mm, source-axis 500 mm, source-detector 1000 mm): forward and
+    reference backprojection element-wise against the reference build (or
+    the restatement when the build is absent)."""
+    vol = nb.ellipsoid_phantom(64, nb.random_ellipsoids(10, 1)).numpy().transpose(2, 1, 0).copy()
+    ang = np.linspace(0, 2 * np.pi, 90, endpoint=False).astype(np.float32)
+    g = nb.ConeBeam((64, 64, 64), ang, 500.0, 1000.0, 128, 2.0, 96, 2.0, size=(128.0, 128.0, 128.0))
+    og = oracle_lib.grid((64, 64, 64), (0, 0, 0), (128.0, 128.0, 128.0))
+    out = ops.cb_forward(torch.from_numpy(vol).to(cuda), g).cpu().numpy()
+    if oracle_lib.have_ref():
+        ref = oracle_lib.ref_cb_forward(og, vol, ang, 500.0, 1000.0, 128, 2.0, 0.5, 96, 2.0, 0.5)
+    else:
+        ref, _ = oracle_lib.cb_forward(og, vol, ang, 500.0, 1000.0, 128, 2.0, 0.5, 96, 2.0, 0.5, use_cosf=True)
+    assert_parity(out, ref)
+    sino = np.ascontiguousarray(ref)
+    bp = ops.cb_backward(torch.from_numpy(sino).to(cuda), g, _lib.REF_BACKPROJECT).cpu().numpy()
+    if oracle_lib.have_ref():
+        rb = oracle_lib.ref_cb_backward(og, sino, ang, 500.0, 1000.0, 128, 2.0, 0.5, 96, 2.0, 0.5)
+    else:
+        rb = oracle_lib.cb_backward(og, sino, ang, 500.0, 1000.0, 128, 2.0, 0.5, 96, 2.0, 0.5, use_cosf=True)
+    assert_parity(bp, rb)
+
+
+def test_lor_pair_vs_fixtures(cuda, golden):
+    lors = torch.from_numpy(golden["lor/lors"]).to(cuda)
+    vol = torch.from_numpy(golden["lor/vol"]).to(cuda)
+    out = ops.lor_forward(lors, vol, (24, 20, 16), size=(48.0, 40.0, 32.0)).cpu().numpy()
+    assert_parity(out, golden["lor/fwd"])
+    assert np.all(out[:5] == 0)
+    vals = torch.from_numpy(golden["lor/vals"]).to(cuda)
+    bp = ops.lor_backward(lors, vals, (24, 20, 16), size=(48.0, 40.0, 32.0)).cpu().numpy()
+    assert_parity(bp, golden["lor/bp"])
+
+
+@pytest.mark.parametrize("flags", [_lib.REF_FORWARD, _lib.TIE_GT])
+def test_driving_axis_tie(cuda, oracle_lib, flags):
+    """Rays with |xd| == |yd| exactly: >= (forward) drives x, > drives y (Q3)."""
+    n = 64
+    t = np.linspace(-9, 9, n).astype(np.float32)
+    lors = np.stack([t - 20, t - 20, np.full(n, 0.7, np.float32), t + 20, t + 20, np.full(n, 3.1, np.float32)])
+    lors = np.ascontiguousarray(lors.astype(np.float32))
+    vol = np.random.default_rng(1).random((16, 16, 16), dtype=np.float32)
+    og = oracle_lib.grid((16, 16, 16), (0, 0, 0), (16.0, 16.0, 16.0))
+    oflags = oracle_lib.INV_L2 | (0 if flags & _lib.TIE_GT else oracle_lib.TIE_GE)
+    ref, _ = oracle_lib.lor_forward(og, vol, lors, flags=oflags)
+    out = ops.lor_forward(torch.from_numpy(lors).to(cuda), torch.from_numpy(vol).to(cuda), (16, 16, 16),
+                          flags=flags).cpu().numpy()
+    assert_parity(out, ref)
+
+
+def test_rays_missing_volume_are_zero(cuda):
+    g = nb.ConeBeam((16, 16, 16), [0.0, 1.0], 100.0, 200.0, 64, 4.0, 8, 1.0, a_shift=40.0)
+    out = ops.cb_forward(torch.ones(g.vol_shape, device=cuda), g)
+    assert float(out.abs().max()) == 0.0
+
+
+def test_linearity_and_adjoint_config2_size(cuda):
+    """Size-independent properties at configuration 2's full size (256^3,
+    360 views, 512x384): linearity, and <Ax,y> = <x,A^T y> in float32."""
+    ang = np.linspace(0, 2 * np.pi, 360, endpoint=False)
+    g = nb.ConeBeam((256, 256, 256), ang, 600.0, 1200.0, 512, 1.2, 384, 1.2, size=(256.0,) * 3)
+    gen = torch.Generator(device=cuda).manual_seed(1)
+    x = torch.rand(g.vol_shape, device=cuda, generator=gen)
+    y = torch.rand(g.sino_shape, device=cuda, generator=gen)
+    ax = ops.cb_forward(x, g, _lib.LINE_INTEGRAL)
+    a2x = ops.cb_forward(2.0 * x, g, _lib.LINE_INTEGRAL)
+    assert float((a2x - 2 * ax).abs().max()) <= 1e-6 * float(ax.abs().max())
+    aty = ops.cb_backward(y, g, _lib.LINE_INTEGRAL)
+    lhs = float((ax.double() * y.double()).sum())
+    rhs = float((x.double() * aty.double()).sum())
+    assert abs(lhs - rhs) / abs(lhs) < 1e-5

@@ -1,0 +1,76 @@
+"""GPU parity of the cpp/deform warp and its derivatives."""
+import numpy as np
+import pytest
+import torch
+
+import nefct_b200 as nb
+from nefct_b200 import ops
+from tests.test_gpu_siddon import assert_parity
+
+pytestmark = pytest.mark.gpu
+
+
+def test_warp_vs_reference_fixture(cuda, golden):
+    t = [torch.from_numpy(golden[k]).to(cuda) for k in ("deform/img", "deform/mx", "deform/my", "deform/mz")]
+    out = ops.warp_forward(*t).cpu().numpy()
+    assert_parity(out, golden["deform/out"], rel=1e-6, mabs=1e-6)
+    # the op-level mirror of Deform(image, mx, my, mz, grid)
+    out2 = nb.cc.deform.deform(*t, [22, 20, 18]).cpu().numpy()
+    np.testing.assert_array_equal(out, out2)
+
+
+def _field(shape, amp, seed, dev, dtype):
+    g = torch.Generator(device=dev).manual_seed(seed)
+    return [(torch.rand(shape, dtype=dtype, device=dev, generator=g) * 2 - 1) * amp for _ in range(3)]
+
+
+def test_warp_adjoint_identity_f64(cuda):
+    shape = (20, 22, 24)
+    m = _field(shape, 3.0, 1, cuda, torch.float64)
+    g = torch.Generator(device=cuda).manual_seed(2)
+    x = torch.randn(shape, dtype=torch.float64, device=cuda, generator=g)
+    y = torch.randn(shape, dtype=torch.float64, device=cuda, generator=g)
+    lhs = float((ops.warp_forward(x, *m) * y).sum())
+    rhs = float((x * ops.warp_adjoint(y, *m)).sum())
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+
+
+def test_warp_dvf_gradient_finite_difference_f64(cuda):
+    shape = (16, 18, 20)
+    m = _field(shape, 2.5, 3, cuda, torch.float64)
+    g = torch.Generator(device=cuda).manual_seed(4)
+    img = torch.rand(shape, dtype=torch.float64, device=cuda, generator=g)
+    w = torch.randn(shape, dtype=torch.float64, device=cuda, generator=g)
+    d = [torch.randn(shape, dtype=torch.float64, device=cuda, generator=g) for _ in range(3)]
+    gx, gy, gz = ops.warp_grad_dvf(img, *m, w)
+    an = float((gx * d[0] + gy * d[1] + gz * d[2]).sum())
+    h = 1e-7
+    fp = float((ops.warp_forward(img, *[a + h * b for a, b in zip(m, d)]) * w).sum())
+    fm = float((ops.warp_forward(img, *[a - h * b for a, b in zip(m, d)]) * w).sum())
+    fd = (fp - fm) / (2 * h)
+    assert abs(fd - an) <= 1e-5 * abs(an)
+
+
+def test_warp_then_project_autograd(cuda):
+    """Gradients w.r.t. image and displacement field through warp -> project,
+    checked by central differences in FP64."""
+    shape = (24, 24, 24)
+    geom = nb.ConeBeam((24, 24, 24), np.linspace(0, 2 * np.pi, 24, endpoint=False), 100.0, 200.0, 40, 1.5, 32, 1.5)
+    gen = torch.Generator(device=cuda).manual_seed(6)
+    img = torch.rand(shape, dtype=torch.float64, device=cuda, generator=gen).requires_grad_()
+    m = [t.requires_grad_() for t in _field(shape, 2.0, 7, cuda, torch.float64)]
+    b = torch.rand(geom.sino_shape, dtype=torch.float64, device=cuda, generator=gen)
+    loss = ((nb.project(nb.warp(img, *m), geom) - b) ** 2).sum()
+    loss.backward()
+    di = torch.randn(shape, dtype=torch.float64, device=cuda, generator=gen)
+    dm = [torch.randn(shape, dtype=torch.float64, device=cuda, generator=gen) for _ in range(3)]
+    an = float((img.grad * di).sum() + sum((t.grad * dd).sum() for t, dd in zip(m, dm)))
+    h = 1e-6
+
+    def f(s):
+        with torch.no_grad():
+            w = ops.warp_forward(img + s * di, *[t + s * dd for t, dd in zip(m, dm)])
+            return float(((ops.cb_forward(w, geom) - b) ** 2).sum())
+
+    fd = (f(h) - f(-h)) / (2 * h)
+    assert abs(fd - an) <= 1e-5 * abs(an)

@@ -4,8 +4,9 @@ Workload (default, the FDK configuration's scanner): 256^3 float32 volume of
 1 mm voxels holding 30 seeded ellipsoids, 360 views over 360 deg, flat
 detector 512 x 384 at 1.2 mm, source-axis 600 mm, source-detector 1200 mm.
 One step = forward projection (reference slab-split weights) of the volume
-plus the exact transpose of the sinogram (what one autograd
-forward+backward of the projector does).
+plus the exact transpose applied to a dense incoming gradient sinogram (what
+one autograd forward+backward of the projector does; a dense gradient has no
+zero rays for the adjoint to skip).
 
 Metric: ray-voxel intersections per second, forward + adjoint (I
 intersections each, I counted exactly by the count kernel).
@@ -224,11 +225,13 @@ def run_gpu(args):
     rays = CFG["nv"] * CFG["na"] * CFG["nb"]
     sino = torch.empty(geom.sino_shape, device=dev)
     back = torch.empty(geom.vol_shape, device=dev)
+    gen = torch.Generator(device=dev).manual_seed(35 + rank)
+    grad = torch.rand(geom.sino_shape, device=dev, generator=gen) + 0.5     # dense incoming gradient
     flush = torch.empty(256 * 2 ** 20 // 4, device=dev)
 
     def step():
         ops.cb_forward(vol, geom, 0, out=sino)
-        ops.cb_backward(sino, geom, 0, out=back)
+        ops.cb_backward(grad, geom, 0, out=back)
 
     for _ in range(args.warmup):
         step()
@@ -244,7 +247,7 @@ def run_gpu(args):
             e0.record()
             ops.cb_forward(vol, geom, 0, out=sino)
             e1.record()
-            ops.cb_backward(sino, geom, 0, out=back)
+            ops.cb_backward(grad, geom, 0, out=back)
             e2.record()
         barrier(ws)
         wall = time.perf_counter() - wall0
@@ -268,7 +271,7 @@ def run_gpu(args):
     for _ in range(args.steps):
         d_in.copy_(h_in, non_blocking=True)
         ops.cb_forward(d_in, geom, 0, out=sino)
-        ops.cb_backward(sino, geom, 0, out=back)
+        ops.cb_backward(grad, geom, 0, out=back)
         h_out.copy_(back, non_blocking=True)
     e1.record()
     barrier(ws)
@@ -321,7 +324,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--views", type=int, default=360, help="views of the scan (360 = the workload; fewer only for profiling)")
     args = ap.parse_args()
+    CFG["nv"] = args.views
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -37,6 +37,11 @@ template <> struct FP<float> {
     static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
     static __device__ __forceinline__ float sqrt(float a) { return __fsqrt_rn(a); }
     static __device__ __forceinline__ int ifloor(float a) { return __float2int_rd(a); }
+    // ratio of a crossing: fast division, error <= 2 ulp
+    static __device__ __forceinline__ float ratio(float a, float b) { return __fdividef(a, b); }
+    static __device__ __forceinline__ float min(float a, float b) { return fminf(a, b); }
+    static __device__ __forceinline__ float max(float a, float b) { return fmaxf(a, b); }
+    static __device__ __forceinline__ float abs(float a) { return fabsf(a); }
 };
 template <> struct FP<double> {
     static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
@@ -45,6 +50,10 @@ template <> struct FP<double> {
     static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
     static __device__ __forceinline__ double sqrt(double a) { return __dsqrt_rn(a); }
     static __device__ __forceinline__ int ifloor(double a) { return __double2int_rd(a); }
+    static __device__ __forceinline__ double ratio(double a, double b) { return __ddiv_rn(a, b); }
+    static __device__ __forceinline__ double min(double a, double b) { return fmin(a, b); }
+    static __device__ __forceinline__ double max(double a, double b) { return fmax(a, b); }
+    static __device__ __forceinline__ double abs(double a) { return fabs(a); }
 };
 
 // Views handled by one launch; the per-view table travels in the kernel's

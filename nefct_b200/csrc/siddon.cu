@@ -57,32 +57,7 @@ __device__ __forceinline__ void cb_ray(const CBParams<T> &p, int ia, int ib, int
     r[5] = F::add(b, off);
 }
 
-template <typename T> struct GatherOp {
-    const T *__restrict__ base;
-    int su, sv, sw;
-    T acc;
-    __device__ __forceinline__ void operator()(int k, int cv, int cw, T r, T W)
-    {
-        acc += __ldg(base + (k * su + cv * sv + cw * sw)) * (r * W);
-    }
-};
-
-template <typename T> struct ScatterOp {
-    T *base;
-    int su, sv, sw;
-    T y;
-    __device__ __forceinline__ void operator()(int k, int cv, int cw, T r, T W)
-    {
-        atomicAdd(base + (k * su + cv * sv + cw * sw), y * (r * W));
-    }
-};
-
-struct CountOp {
-    unsigned n;
-    template <typename T> __device__ __forceinline__ void operator()(int, int, int, T, T) { ++n; }
-};
-
-template <typename T>
+template <typename T, bool DIV>
 __global__ void __launch_bounds__(256) cb_forward_kernel(const __grid_constant__ CBParams<T> p)
 {
     const int ia = blockIdx.x * 32 + threadIdx.x;
@@ -94,19 +69,15 @@ __global__ void __launch_bounds__(256) cb_forward_kernel(const __grid_constant__
     Walk<T> w;
     T acc = (T)0;
     if (setup_walk(p.g, r, p.flags, w)) {
-        GatherOp<T> op;
-        op.sw = p.g.nx * p.g.ny;
-        if (!w.xdrive) { op.base = p.vol; op.su = p.g.nx; op.sv = 1; }
-        else if (p.volT) { op.base = p.volT; op.su = p.g.ny; op.sv = 1; }
-        else { op.base = p.vol; op.su = 1; op.sv = p.g.nx; }
-        op.acc = (T)0;
-        run_walk(w, p.g, op);
-        acc = op.acc;
+        const int sw = p.g.nx * p.g.ny;
+        if (!w.xdrive) acc = gather_walk<T, DIV, true, false>(w, p.g, p.vol, p.g.nx, 1, sw);
+        else if (p.volT) acc = gather_walk<T, DIV, true, false>(w, p.g, p.volT, p.g.ny, 1, sw);
+        else acc = gather_walk<T, DIV, false, false>(w, p.g, p.vol, 1, p.g.nx, sw);
     }
     p.out[(size_t)(p.v0 + iv) * p.na * p.nb + (size_t)ib * p.na + ia] = acc;
 }
 
-template <typename T>
+template <typename T, bool DIV>
 __global__ void __launch_bounds__(256) cb_backward_kernel(const __grid_constant__ CBParams<T> p)
 {
     const int ia = blockIdx.x * 32 + threadIdx.x;
@@ -124,15 +95,13 @@ __global__ void __launch_bounds__(256) cb_backward_kernel(const __grid_constant_
     cb_ray(p, ia, ib, iv, r);
     Walk<T> w;
     if (!setup_walk(p.g, r, p.flags, w)) return;
-    ScatterOp<T> op;
-    op.sw = p.g.nx * p.g.ny;
-    op.y = y;
-    if (!w.xdrive) { op.base = p.out; op.su = p.g.nx; op.sv = 1; }
-    else if (p.outT) { op.base = p.outT; op.su = p.g.ny; op.sv = 1; }
-    else { op.base = p.out; op.su = 1; op.sv = p.g.nx; }
-    run_walk(w, p.g, op);
+    const int sw = p.g.nx * p.g.ny;
+    if (!w.xdrive) scatter_walk<T, DIV, true, false>(w, p.g, p.out, p.g.nx, 1, sw, y);
+    else if (p.outT) scatter_walk<T, DIV, true, false>(w, p.g, p.outT, p.g.ny, 1, sw, y);
+    else scatter_walk<T, DIV, false, false>(w, p.g, p.out, 1, p.g.nx, sw, y);
 }
 
+template <bool DIV>
 __global__ void __launch_bounds__(256) cb_count_kernel(const __grid_constant__ CBParams<float> p)
 {
     const int ia = blockIdx.x * 32 + threadIdx.x;
@@ -143,11 +112,7 @@ __global__ void __launch_bounds__(256) cb_count_kernel(const __grid_constant__ C
         float r[6];
         cb_ray(p, ia, ib, iv, r);
         Walk<float> w;
-        if (setup_walk(p.g, r, p.flags, w)) {
-            CountOp op{0};
-            run_walk(w, p.g, op);
-            n = op.n;
-        }
+        if (setup_walk(p.g, r, p.flags, w)) n = count_walk<float, DIV>(w, p.g);
     }
     for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
     if ((threadIdx.x & 31) == 0 && n) atomicAdd(p.count, (unsigned long long)n);
@@ -203,7 +168,7 @@ template <typename T> struct LorParams {
     T *out;
 };
 
-template <typename T>
+template <typename T, bool DIV, bool Q5>
 __global__ void __launch_bounds__(256) lor_forward_kernel(const __grid_constant__ LorParams<T> p)
 {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < p.n;
@@ -213,17 +178,15 @@ __global__ void __launch_bounds__(256) lor_forward_kernel(const __grid_constant_
         Walk<T> w;
         T acc = (T)0;
         if (setup_walk(p.g, r, p.flags, w)) {
-            GatherOp<T> op;
-            op.base = p.vol; op.sw = p.g.nx * p.g.ny; op.acc = (T)0;
-            if (w.xdrive) { op.su = 1; op.sv = p.g.nx; } else { op.su = p.g.nx; op.sv = 1; }
-            run_walk(w, p.g, op);
-            acc = op.acc;
+            const int sw = p.g.nx * p.g.ny;
+            acc = w.xdrive ? gather_walk<T, DIV, false, Q5>(w, p.g, p.vol, 1, p.g.nx, sw)
+                           : gather_walk<T, DIV, true, Q5>(w, p.g, p.vol, p.g.nx, 1, sw);
         }
         p.out[i] = acc;
     }
 }
 
-template <typename T>
+template <typename T, bool DIV, bool Q5>
 __global__ void __launch_bounds__(256) lor_backward_kernel(const __grid_constant__ LorParams<T> p)
 {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < p.n;
@@ -234,14 +197,16 @@ __global__ void __launch_bounds__(256) lor_backward_kernel(const __grid_constant
         for (int j = 0; j < 6; ++j) r[j] = p.lors[j * p.n + i];
         Walk<T> w;
         if (!setup_walk(p.g, r, p.flags, w)) continue;
-        ScatterOp<T> op;
-        op.base = p.out; op.sw = p.g.nx * p.g.ny; op.y = y;
-        if (w.xdrive) { op.su = 1; op.sv = p.g.nx; } else { op.su = p.g.nx; op.sv = 1; }
-        run_walk(w, p.g, op);
+        const int sw = p.g.nx * p.g.ny;
+        if (w.xdrive) scatter_walk<T, DIV, false, Q5>(w, p.g, p.out, 1, p.g.nx, sw, y);
+        else scatter_walk<T, DIV, true, Q5>(w, p.g, p.out, p.g.nx, 1, sw, y);
     }
 }
 
 // ---------------- host side ----------------
+
+// The walk skips its divisions when both transverse pitches equal the x pitch.
+template <typename T> static bool cubic(const GridDev<T> &g) { return g.dy == (T)1 && g.dz == (T)1; }
 
 static const uint32_t kWalkFlags = NEFCT_TIE_GT | NEFCT_SKIP_SHORT | NEFCT_NO_INV_L2 | NEFCT_Q5 |
                                    NEFCT_Q8_INDEX | NEFCT_NO_TRANSPOSE;
@@ -345,7 +310,8 @@ static nefct_status cb_forward_impl(const nefct_cb_geom *g, const T *vol, T *sin
         const int nvc = std::min(kMax, g->nv - v0);
         fill_views(*p, g, v0, nvc);
         dim3 grid((g->na + 31) / 32, (g->nb + 7) / 8, nvc);
-        cb_forward_kernel<T><<<grid, dim3(32, 8), 0, s>>>(*p);
+        if (cubic(p->g)) cb_forward_kernel<T, false><<<grid, dim3(32, 8), 0, s>>>(*p);
+        else cb_forward_kernel<T, true><<<grid, dim3(32, 8), 0, s>>>(*p);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) { delete p; return cuda_fail(e, "cb_forward_kernel"); }
     }
@@ -378,7 +344,8 @@ static nefct_status cb_backward_impl(const nefct_cb_geom *g, const T *sino, T *v
         const int nvc = std::min(kMax, g->nv - v0);
         fill_views(*p, g, v0, nvc);
         dim3 grid((g->na + 31) / 32, (g->nb + 7) / 8, nvc);
-        cb_backward_kernel<T><<<grid, dim3(32, 8), 0, s>>>(*p);
+        if (cubic(p->g)) cb_backward_kernel<T, false><<<grid, dim3(32, 8), 0, s>>>(*p);
+        else cb_backward_kernel<T, true><<<grid, dim3(32, 8), 0, s>>>(*p);
         e = cudaGetLastError();
         if (e != cudaSuccess) { delete p; return cuda_fail(e, "cb_backward_kernel"); }
     }
@@ -414,8 +381,17 @@ static nefct_status lor_impl(const nefct_grid *grid, const T *lors, int64_t n, c
     }
     if (n == 0) return NEFCT_OK;
     const long long blocks = std::min<long long>((n + 255) / 256, 148ll * 64);
-    if (forward) lor_forward_kernel<T><<<(unsigned)blocks, 256, 0, s>>>(p);
-    else lor_backward_kernel<T><<<(unsigned)blocks, 256, 0, s>>>(p);
+    const bool q5 = (flags & NEFCT_Q5) != 0, cub = cubic(p.g);
+#define NEFCT_LOR_LAUNCH(K)                                                              \
+    do {                                                                                 \
+        if (cub && !q5) K<T, false, false><<<(unsigned)blocks, 256, 0, s>>>(p);          \
+        else if (cub) K<T, false, true><<<(unsigned)blocks, 256, 0, s>>>(p);             \
+        else if (!q5) K<T, true, false><<<(unsigned)blocks, 256, 0, s>>>(p);             \
+        else K<T, true, true><<<(unsigned)blocks, 256, 0, s>>>(p);                       \
+    } while (0)
+    if (forward) NEFCT_LOR_LAUNCH(lor_forward_kernel);
+    else NEFCT_LOR_LAUNCH(lor_backward_kernel);
+#undef NEFCT_LOR_LAUNCH
     NEFCT_CHECK_LAUNCH(forward ? "lor_forward_kernel" : "lor_backward_kernel");
     return NEFCT_OK;
 }
@@ -472,7 +448,8 @@ nefct_status nefct_cb_count_intersections(const nefct_cb_geom *g, uint32_t flags
         const int nvc = std::min(kMax, g->nv - v0);
         fill_views(*p, g, v0, nvc);
         dim3 grid((g->na + 31) / 32, (g->nb + 7) / 8, nvc);
-        cb_count_kernel<<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>(*p);
+        if (cubic(p->g)) cb_count_kernel<false><<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>(*p);
+        else cb_count_kernel<true><<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>(*p);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) { delete p; return cuda_fail(e, "cb_count_kernel"); }
     }

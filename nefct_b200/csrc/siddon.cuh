@@ -19,7 +19,13 @@
 //    the volume (with a one-voxel margin); slabs outside contribute nothing,
 //    so the clip changes no result, only the trip count;
 //  * the three-way case split is written as one predicated sequence of at
-//    most three (voxel, weight) slots, in the reference's accumulation order.
+//    most three (voxel, weight) slots, in the reference's accumulation order;
+//  * the crossing ratios use the fast division (<= 2 ulp) in FP32: they only
+//    scale weights, and the split is continuous in them;
+//  * the per-ray weight W is applied once to the ray's sum of value * ratio
+//    (rounding-level difference from the per-contribution products);
+//  * slabs whose candidate voxels are all inside the grid skip the range
+//    checks (interior range computed with the clip).
 #pragma once
 
 #include "common.cuh"
@@ -52,27 +58,40 @@ template <typename T> struct Walk {
     T dv, nu2, nv2;
     T W, Wmid;           // contribution weights (Wmid: three-voxel middle slot, Q5)
     int nu, nv, k0, k1;  // slab count, transverse extent, inclusive slab range
+    int ki0, ki1;        // interior slabs: every candidate voxel is inside the grid
     bool xdrive, vdiv;
 };
 
-// Clips the slab range of the driving axis to [k0, k1] (FP64): slab k lies
-// between planes t = k - nu2 and t + 1; position p(t) = A + B t must reach
-// [-1, n + 1] for the slab to be able to touch the volume.
-__device__ __forceinline__ void clip_axis(double A, double B, int n, double nu2, int nu, int &k0, int &k1)
+// Slab ranges of the driving axis (FP64).  Slab k lies between planes
+// t = k - nu2 and t + 1, and the transverse position is p(t) = A + B t.
+// [k0, k1]: slabs whose positions reach [-1 - m, n + 1 + m], i.e. that can
+// touch the grid.  [ki0, ki1]: slabs whose positions at both planes lie in
+// [m, n - m], so the floors of both planes are valid indices and no range
+// check is needed.  m covers the difference between these FP64 positions and
+// the FP32 ones the walk evaluates: 1/64 voxel plus 1e-5 of the largest
+// magnitude entering them (a few hundred FP32 ulps).
+__device__ __forceinline__ void clip_axis(double A, double B, int n, double nu2, int nu, double mag, int &k0,
+                                          int &k1, int &ki0, int &ki1)
 {
-    const double lo = -1.0, hi = (double)n + 1.0;
+    const double m = 1.0 / 64.0 + 1e-5 * mag;
     if (B == 0.0) {
-        if (A < lo || A > hi) { k0 = 1; k1 = 0; }
+        if (A < -1.0 - m || A > (double)n + 1.0 + m) { k0 = 1; k1 = 0; }
+        if (A < m || A > (double)n - m) { ki0 = 1; ki1 = 0; }
         return;
     }
-    double t0 = (lo - A) / B, t1 = (hi - A) / B;
-    if (t0 > t1) { const double s = t0; t0 = t1; t1 = s; }
-    // k >= t0 + nu2 - 1 and k <= t1 + nu2; clamp before converting
-    double a = ceil(t0 + nu2 - 1.0), b = floor(t1 + nu2);
-    a = fmin(fmax(a, -1.0), (double)nu + 1.0);
-    b = fmax(fmin(b, (double)nu), -2.0);
-    k0 = max(k0, (int)a);
-    k1 = min(k1, (int)b);
+    auto span = [&](double lo, double hi, double &t0, double &t1) {
+        t0 = (lo - A) / B;
+        t1 = (hi - A) / B;
+        if (t0 > t1) { const double s = t0; t0 = t1; t1 = s; }
+    };
+    auto clampk = [&](double v) { return (int)fmin(fmax(v, -2.0), (double)nu + 1.0); };
+    double t0, t1;
+    span(-1.0 - m, (double)n + 1.0 + m, t0, t1);
+    k0 = max(k0, clampk(ceil(t0 + nu2 - 1.0)));
+    k1 = min(k1, clampk(floor(t1 + nu2)));
+    span(m, (double)n - m, t0, t1);
+    ki0 = max(ki0, clampk(ceil(t0 + nu2)));
+    ki1 = min(ki1, clampk(floor(t1 + nu2) - 1.0));
 }
 
 // Per-ray setup of project_device / backproject_device (reference :19-44,
@@ -110,64 +129,208 @@ __device__ __forceinline__ bool setup_walk(const GridDev<T> &g, const T *r, uint
     w.Wmid = ((flags & NEFCT_Q5) && !w.xdrive) ? F::div(W, L) : W;
 
     w.k0 = 0; w.k1 = w.nu - 1;
+    w.ki0 = 0; w.ki1 = w.nu - 1;
     const double pu = (double)w.pu, kv = (double)w.kv, kw = (double)w.kw;
     const double dv = (double)w.dv, dz = (double)g.dz;
-    clip_axis(((double)w.pv - kv * pu) / dv + (double)w.nv2, kv / dv, w.nv, (double)w.nu2, w.nu, w.k0, w.k1);
-    clip_axis(((double)w.pw - kw * pu) / dz + (double)g.nz2, kw / dz, g.nz, (double)w.nu2, w.nu, w.k0, w.k1);
+    const double mag = fabs(pu) + fabs((double)w.pv) + fabs((double)w.pw) + (double)(w.nu + w.nv + g.nz);
+    clip_axis(((double)w.pv - kv * pu) / dv + (double)w.nv2, kv / dv, w.nv, (double)w.nu2, w.nu, mag, w.k0, w.k1,
+              w.ki0, w.ki1);
+    clip_axis(((double)w.pw - kw * pu) / dz + (double)g.nz2, kw / dz, g.nz, (double)w.nu2, w.nu, mag, w.k0, w.k1,
+              w.ki0, w.ki1);
     w.k0 = max(w.k0, 0);
     w.k1 = min(w.k1, w.nu - 1);
+    w.ki0 = max(w.ki0, w.k0);
+    w.ki1 = min(w.ki1, w.k1);
     return w.k0 <= w.k1;
 }
 
-// Visits every (slab, v, z, ratio, weight) contribution of the ray in the
-// reference's order.  op(k, cv, cw, r, Wslot) is called for admitted voxels.
-template <typename T, class Op>
-__device__ __forceinline__ void run_walk(const Walk<T> &w, const GridDev<T> &g, Op &op)
-{
+// The up-to-three contributions of one driving slab: flat volume index,
+// split ratio r (the weight is r * W) and activity, in the reference's order.
+template <typename T> struct SlabSlots {
+    int idx[3];
+    T r[3];
+    bool ok[3];
+    bool mid3;          // slot 1 is the middle entry of a three-voxel split (Q5)
+};
+
+// Walks the slabs of one ray, carrying the plane positions, their floors and
+// the z row offsets from one slab to the next.
+//   DIV   the grid is not cubic: positions divide by dy (x-driven) / dz;
+//   SWP   the z slope is >= 0 (uniform along a detector row, so along a warp);
+//   SV1   the transverse stride is 1 (x-fastest volume for y-driven rays,
+//         y-fastest copy for x-driven rays).
+// next<CHECK>() returns the next slab's contributions; CHECK=false is only
+// valid for interior slabs, where all candidate voxels are inside the grid.
+template <typename T, bool DIV, bool SWP, bool SV1> struct Walker {
     using F = FP<T>;
-    const bool sv = w.kv >= (T)0, sw = w.kw >= (T)0;
-    const bool zdiv = g.dz != (T)1;
-    const int nv = w.nv, nz = g.nz;
-    auto posv = [&](T t) {
-        T q = F::add(w.pv, F::mul(w.kv, F::sub(t, w.pu)));
-        if (w.vdiv) q = F::div(q, w.dv);
-        return F::add(q, w.nv2);
-    };
-    auto posw = [&](T t) {
-        T q = F::add(w.pw, F::mul(w.kw, F::sub(t, w.pu)));
-        if (zdiv) q = F::div(q, g.dz);
-        return F::add(q, g.nz2);
-    };
-    T t = F::sub((T)w.k0, w.nu2);
-    T qav = posv(t), qaw = posw(t);
-    int fav = F::ifloor(qav), faw = F::ifloor(qaw);
-    for (int k = w.k0; k <= w.k1; ++k) {
+    T pu, pv, pw, kv, kw, dv, dz, nv2, nz2;
+    int nv, nz, su, sv, sw, base;
+    bool vdiv, zdiv;
+    T t, qav, qaw;
+    int fav, faw, rowa;
+
+    __device__ __forceinline__ T posv(T tt) const
+    {
+        T q = F::add(pv, F::mul(kv, F::sub(tt, pu)));
+        if (DIV && vdiv) q = F::div(q, dv);
+        return F::add(q, nv2);
+    }
+    __device__ __forceinline__ T posw(T tt) const
+    {
+        T q = F::add(pw, F::mul(kw, F::sub(tt, pu)));
+        if (DIV && zdiv) q = F::div(q, dz);
+        return F::add(q, nz2);
+    }
+
+    __device__ __forceinline__ Walker(const Walk<T> &w, const GridDev<T> &g, int k, int su_, int sv_, int sw_)
+    {
+        pu = w.pu; pv = w.pv; pw = w.pw; kv = w.kv; kw = w.kw; dv = w.dv; dz = g.dz;
+        nv2 = w.nv2; nz2 = g.nz2;
+        nv = w.nv; nz = g.nz; su = su_; sv = SV1 ? 1 : sv_; sw = sw_;
+        vdiv = w.vdiv;
+        zdiv = dz != (T)1;
+        base = k * su;
+        t = F::sub((T)k, w.nu2);
+        qav = posv(t);
+        qaw = posw(t);
+        fav = F::ifloor(qav);
+        faw = F::ifloor(qaw);
+        rowa = faw * sw;
+    }
+
+    template <bool CHECK> __device__ __forceinline__ SlabSlots<T> next()
+    {
         const T t2 = F::add(t, (T)1);
         const T qbv = posv(t2), qbw = posw(t2);
         const int fbv = F::ifloor(qbv), fbw = F::ifloor(qbw);
-        const T q1v = sv ? qav : qbv, q2v = sv ? qbv : qav;
-        const T q1w = sw ? qaw : qbw, q2w = sw ? qbw : qaw;
-        const int cv1 = sv ? fav : fbv, cv2 = sv ? fbv : fav;
-        const int cw1 = sw ? faw : fbw, cw2 = sw ? fbw : faw;
-        t = t2; qav = qbv; qaw = qbw; fav = fbv; faw = fbw;
+        const int rowb = fbw * sw;
+        // low/high plane of the slab in v (min/max equals the slope-sign choice)
+        const T q1v = F::min(qav, qbv), q2v = F::max(qav, qbv);
+        const int cv1 = min(fav, fbv), cv2 = max(fav, fbv);
+        const T q1w = SWP ? qaw : qbw, q2w = SWP ? qbw : qaw;
+        const int cw1 = SWP ? faw : fbw, cw2 = SWP ? fbw : faw;
+        const int row1 = SWP ? rowa : rowb, row2 = SWP ? rowb : rowa;
+        const int b = base;
+        t = t2; qav = qbv; qaw = qbw; fav = fbv; faw = fbw; rowa = rowb; base += su;
 
         const bool vx = cv1 != cv2, wx = cw1 != cw2;
-        // slab admission (reference :80, :92, :112, :116, :132)
-        if (cv1 >= nv || cv1 < (vx ? -1 : 0) || cw1 >= nz || cw1 < (wx ? -1 : 0)) continue;
-        T rv = (T)1, rw = (T)1;
-        if (vx) rv = F::div(F::sub((T)cv2, q1v), F::sub(q2v, q1v));
-        if (wx) rw = F::div(F::sub((T)cw2, q1w), F::sub(q2w, q1w));
+        const T rvq = F::ratio(F::sub((T)cv2, q1v), F::sub(q2v, q1v));
+        const T rwq = F::ratio(F::sub((T)cw2, q1w), F::sub(q2w, q1w));
+        const T rv = vx ? rvq : (T)1, rw = wx ? rwq : (T)1;
         const bool vfirst = rv > rw;   // middle voxel (cv1, cw2) when true, else (cv2, cw1)
-        if (cv1 >= 0 && cw1 >= 0) op(k, cv1, cw1, vfirst ? rw : rv, w.W);
-        if (vx || wx) {
+        SlabSlots<T> s;
+        s.r[0] = F::min(rv, rw);
+        s.r[1] = F::abs(F::sub(rv, rw));
+        s.r[2] = F::sub((T)1, F::max(rv, rw));
+        s.idx[0] = b + cv1 * sv + row1;
+        s.idx[1] = b + (vfirst ? cv1 * sv + row2 : cv2 * sv + row1);
+        s.idx[2] = b + cv2 * sv + row2;
+        s.mid3 = vx && wx;
+        if (CHECK) {
+            // slab admission (reference :80, :92, :112, :116, :132)
+            const bool adm = (unsigned)(cv1 + (int)vx) < (unsigned)(nv + (int)vx) &&
+                             (unsigned)(cw1 + (int)wx) < (unsigned)(nz + (int)wx);
             const int mv = vfirst ? cv1 : cv2, mw = vfirst ? cw2 : cw1;
-            const T rm = vfirst ? F::sub(rv, rw) : F::sub(rw, rv);
-            if ((unsigned)mv < (unsigned)nv && (unsigned)mw < (unsigned)nz)
-                op(k, mv, mw, rm, (vx && wx) ? w.Wmid : w.W);
-            if (vx && wx && cv2 < nv && cw2 < nz)
-                op(k, cv2, cw2, F::sub((T)1, vfirst ? rv : rw), w.W);
+            s.ok[0] = adm && (cv1 | cw1) >= 0;
+            s.ok[1] = adm && (vx || wx) && (unsigned)mv < (unsigned)nv && (unsigned)mw < (unsigned)nz;
+            s.ok[2] = adm && vx && wx && cv2 < nv && cw2 < nz;
+        } else {
+            s.ok[0] = true;
+            s.ok[1] = vx || wx;
+            s.ok[2] = vx && wx;
         }
+        return s;
     }
+};
+
+// Runs f(slots) over slabs [a, b] with the given check mode.
+template <bool CHECK, class WK, class Fn>
+__device__ __forceinline__ void walk_range(WK &it, int a, int b, Fn &f)
+{
+    for (int k = a; k <= b; ++k) f(it.template next<CHECK>());
+}
+
+// Visits the slabs k0..k1 of a ray: boundary slabs with range checks,
+// interior slabs without.
+template <class WK, class Fn>
+__device__ __forceinline__ void walk_all(WK &it, const int k0, const int k1, const int ki0, const int ki1, Fn &f)
+{
+    if (ki0 <= ki1) {
+        walk_range<true>(it, k0, ki0 - 1, f);
+        walk_range<false>(it, ki0, ki1, f);
+        walk_range<true>(it, ki1 + 1, k1, f);
+    } else {
+        walk_range<true>(it, k0, k1, f);
+    }
+}
+
+// Weighted sum of the volume along the ray (forward):
+//   sum over contributions of v * r, times W (and Wmid for Q5 middles).
+template <typename T, bool DIV, bool SWP, bool SV1, bool Q5>
+__device__ __forceinline__ T gather_walk_t(const Walk<T> &w, const GridDev<T> &g, const T *__restrict__ base,
+                                           int su, int sv, int sw)
+{
+    Walker<T, DIV, SWP, SV1> it(w, g, w.k0, su, sv, sw);
+    T acc = (T)0, accm = (T)0;
+    auto f = [&](const SlabSlots<T> &s) {
+        const T v0 = s.ok[0] ? __ldg(base + s.idx[0]) : (T)0;
+        const T v1 = s.ok[1] ? __ldg(base + s.idx[1]) : (T)0;
+        const T v2 = s.ok[2] ? __ldg(base + s.idx[2]) : (T)0;
+        acc += v0 * s.r[0];
+        if (Q5 && s.mid3) accm += v1 * s.r[1];
+        else acc += v1 * s.r[1];
+        acc += v2 * s.r[2];
+    };
+    walk_all(it, w.k0, w.k1, w.ki0, w.ki1, f);
+    return Q5 ? acc * w.W + accm * w.Wmid : acc * w.W;
+}
+
+template <typename T, bool DIV, bool SV1, bool Q5>
+__device__ __forceinline__ T gather_walk(const Walk<T> &w, const GridDev<T> &g, const T *__restrict__ base, int su,
+                                         int sv, int sw)
+{
+    return w.kw >= (T)0 ? gather_walk_t<T, DIV, true, SV1, Q5>(w, g, base, su, sv, sw)
+                        : gather_walk_t<T, DIV, false, SV1, Q5>(w, g, base, su, sv, sw);
+}
+
+// Scatters value * weight along the ray (transpose); reductions do not wait
+// for their result.
+template <typename T, bool DIV, bool SWP, bool SV1, bool Q5>
+__device__ __forceinline__ void scatter_walk_t(const Walk<T> &w, const GridDev<T> &g, T *base, int su, int sv,
+                                               int sw, T value)
+{
+    Walker<T, DIV, SWP, SV1> it(w, g, w.k0, su, sv, sw);
+    const T yw = value * w.W, ym = value * w.Wmid;
+    auto f = [&](const SlabSlots<T> &s) {
+        if (s.ok[0]) atomicAdd(base + s.idx[0], yw * s.r[0]);
+        if (s.ok[1]) atomicAdd(base + s.idx[1], ((Q5 && s.mid3) ? ym : yw) * s.r[1]);
+        if (s.ok[2]) atomicAdd(base + s.idx[2], yw * s.r[2]);
+    };
+    walk_all(it, w.k0, w.k1, w.ki0, w.ki1, f);
+}
+
+template <typename T, bool DIV, bool SV1, bool Q5>
+__device__ __forceinline__ void scatter_walk(const Walk<T> &w, const GridDev<T> &g, T *base, int su, int sv, int sw,
+                                             T value)
+{
+    if (w.kw >= (T)0) scatter_walk_t<T, DIV, true, SV1, Q5>(w, g, base, su, sv, sw, value);
+    else scatter_walk_t<T, DIV, false, SV1, Q5>(w, g, base, su, sv, sw, value);
+}
+
+// Number of contributions of the ray (the throughput unit).
+template <typename T, bool DIV>
+__device__ __forceinline__ unsigned count_walk(const Walk<T> &w, const GridDev<T> &g)
+{
+    unsigned n = 0;
+    auto f = [&](const SlabSlots<T> &s) { n += (unsigned)s.ok[0] + (unsigned)s.ok[1] + (unsigned)s.ok[2]; };
+    if (w.kw >= (T)0) {
+        Walker<T, DIV, true, true> it(w, g, w.k0, 0, 1, 0);
+        walk_all(it, w.k0, w.k1, w.ki0, w.ki1, f);
+    } else {
+        Walker<T, DIV, false, true> it(w, g, w.k0, 0, 1, 0);
+        walk_all(it, w.k0, w.k1, w.ki0, w.ki1, f);
+    }
+    return n;
 }
 
 }  // namespace nefct

@@ -41,6 +41,21 @@ const char *nefct_version(void);
 const char *nefct_status_string(nefct_status st);
 const char *nefct_last_error(void);
 
+/* Process-wide launch tuning used by the autotuner (nefct_b200/autotune.py).
+ * No counterpart in the reference (its launch shapes are constants,
+ * siddon.cu.cc:8-10).  Every value runs the same per-ray arithmetic: the
+ * forward's output is bitwise independent of it; the transpose sums with
+ * atomics, whose order is not fixed under any setting.
+ *   NEFCT_TUNE_CB_ROWS   detector rows per CTA of the cone-beam Siddon
+ *                        kernels (1, 2, 4, 8; 32 columns per row); default 8
+ *   NEFCT_TUNE_CB_ORDER  0: row bands outermost (default; keeps the volume
+ *                        slab of the rows in flight in L2), 1: views outermost */
+#define NEFCT_TUNE_CB_ROWS  0
+#define NEFCT_TUNE_CB_ORDER 1
+#define NEFCT_TUNE_COUNT    2
+nefct_status nefct_tune_set(int32_t key, int32_t value);
+int32_t nefct_tune_get(int32_t key);
+
 /* Voxel grid: nx*ny*nz voxels of a box of extent (sx, sy, sz) centred on
  * (cx, cy, cz).  Same meaning as the reference ops' grid/center/size inputs
  * (nefct/cc/siddon_3d/siddon.cc:13-15; cpp/siddon/siddon_gpu.cc:14-16),

@@ -29,6 +29,7 @@ LOR_REF_BACKPROJECT = TIE_GT | SKIP_SHORT | NO_INV_L2
 FDK_NO_WEIGHT = 0x100
 
 DET_FLAT, DET_CYL = 0, 1
+TUNE_CB_ROWS, TUNE_CB_ORDER = 0, 1
 WIN_RAM_LAK, WIN_SHEPP_LOGAN, WIN_COSINE, WIN_HAMMING, WIN_HANN = 0, 1, 2, 3, 4
 WINDOWS = {"ram-lak": WIN_RAM_LAK, "shepp-logan": WIN_SHEPP_LOGAN, "cosine": WIN_COSINE,
            "hamming": WIN_HAMMING, "hann": WIN_HANN}
@@ -64,6 +65,8 @@ _PROTOS = {
     "nefct_version": (C.c_char_p, []),
     "nefct_status_string": (C.c_char_p, [_i32]),
     "nefct_last_error": (C.c_char_p, []),
+    "nefct_tune_set": (_i32, [_i32, _i32]),
+    "nefct_tune_get": (_i32, [_i32]),
     "nefct_cb_workspace_bytes": (C.c_size_t, [C.POINTER(CBGeom), _u32]),
     "nefct_cb_forward": (_i32, [C.POINTER(CBGeom), _vp, _vp, _u32, _vp, C.c_size_t, _vp]),
     "nefct_cb_backward": (_i32, [C.POINTER(CBGeom), _vp, _vp, _u32, _vp, C.c_size_t, _vp]),

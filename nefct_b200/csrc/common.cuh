@@ -9,6 +9,9 @@
 
 namespace nefct {
 
+// Process-wide launch tuning (nefct_tune_set / nefct_tune_get).
+int tune_get(int key);
+
 // Records a message for nefct_last_error() and returns the status.
 nefct_status fail(nefct_status st, const char *fmt, ...);
 // Maps a CUDA error to NEFCT_ERR_CUDA with the call site in the message.
@@ -54,6 +57,27 @@ template <> struct FP<double> {
     static __device__ __forceinline__ double min(double a, double b) { return fmin(a, b); }
     static __device__ __forceinline__ double max(double a, double b) { return fmax(a, b); }
     static __device__ __forceinline__ double abs(double a) { return fabs(a); }
+};
+
+// Pairs of values updated by the same operation sequence (the two
+// transverse plane positions).  FP32 uses the paired sm_100 instructions,
+// which round each component exactly like the scalar _rn operation.
+template <typename T> struct Pair;
+template <> struct Pair<float> {
+    float2 v;
+    static __device__ __forceinline__ Pair make(float a, float b) { Pair p; p.v = make_float2(a, b); return p; }
+    __device__ __forceinline__ float x() const { return v.x; }
+    __device__ __forceinline__ float y() const { return v.y; }
+    static __device__ __forceinline__ Pair add(Pair a, Pair b) { Pair p; p.v = __fadd2_rn(a.v, b.v); return p; }
+    static __device__ __forceinline__ Pair mul(Pair a, Pair b) { Pair p; p.v = __fmul2_rn(a.v, b.v); return p; }
+};
+template <> struct Pair<double> {
+    double a_, b_;
+    static __device__ __forceinline__ Pair make(double a, double b) { Pair p; p.a_ = a; p.b_ = b; return p; }
+    __device__ __forceinline__ double x() const { return a_; }
+    __device__ __forceinline__ double y() const { return b_; }
+    static __device__ __forceinline__ Pair add(Pair a, Pair b) { return make(__dadd_rn(a.a_, b.a_), __dadd_rn(a.b_, b.b_)); }
+    static __device__ __forceinline__ Pair mul(Pair a, Pair b) { return make(__dmul_rn(a.a_, b.a_), __dmul_rn(a.b_, b.b_)); }
 };
 
 // Views handled by one launch; the per-view table travels in the kernel's

@@ -3,7 +3,11 @@
 //
 // Launch shape: one thread per ray; a 256-thread CTA covers 32 adjacent
 // detector columns x 8 rows of one view, so each warp is 32 neighbouring
-// columns of one row.  Neighbouring rays of a warp cross a driving slab at
+// columns of one row.  The grid runs (column tile, view, row band) with the
+// row band slowest: the CTAs in flight cover all views of one band of rows,
+// whose rays only reach a thin z-slab of the volume, so the gathered volume
+// (forward) or the reduced accumulator (transpose) stays resident in L2
+// instead of every view sweeping the whole volume through it.  Neighbouring rays of a warp cross a driving slab at
 // neighbouring transverse positions; with the transverse axis contiguous in
 // memory a warp's gather touches one or two 128-byte lines.  That holds for
 // y-driven rays in the x-fastest volume; x-driven rays read a y-fastest copy
@@ -20,7 +24,7 @@ template <typename T> struct CBParams {
     GridDev<T> g;
     int na, nb, nvc, v0, nv_total;
     T src_iso, src_det, da, ai, db, bi, half_a, half_b;
-    int cyl;
+    int cyl, band_major;
     uint32_t flags;
     const T *vol;        // x-fastest volume (forward source)
     const T *volT;       // y-fastest copy for x-driven rays, or nullptr
@@ -57,12 +61,22 @@ __device__ __forceinline__ void cb_ray(const CBParams<T> &p, int ia, int ib, int
     r[5] = F::add(b, off);
 }
 
+// Detector cell of this thread: 32 columns x blockDim.y rows per CTA; grid
+// (column tile, view, row band) when band_major, else (column tile, row
+// band, view).
+template <typename T>
+__device__ __forceinline__ void cb_cell(const CBParams<T> &p, int &ia, int &ib, int &iv)
+{
+    ia = blockIdx.x * 32 + threadIdx.x;
+    if (p.band_major) { iv = blockIdx.y; ib = blockIdx.z * blockDim.y + threadIdx.y; }
+    else { ib = blockIdx.y * blockDim.y + threadIdx.y; iv = blockIdx.z; }
+}
+
 template <typename T, bool DIV>
 __global__ void __launch_bounds__(256) cb_forward_kernel(const __grid_constant__ CBParams<T> p)
 {
-    const int ia = blockIdx.x * 32 + threadIdx.x;
-    const int ib = blockIdx.y * 8 + threadIdx.y;
-    const int iv = blockIdx.z;
+    int ia, ib, iv;
+    cb_cell(p, ia, ib, iv);
     if (ia >= p.na || ib >= p.nb) return;
     T r[6];
     cb_ray(p, ia, ib, iv, r);
@@ -80,9 +94,8 @@ __global__ void __launch_bounds__(256) cb_forward_kernel(const __grid_constant__
 template <typename T, bool DIV>
 __global__ void __launch_bounds__(256) cb_backward_kernel(const __grid_constant__ CBParams<T> p)
 {
-    const int ia = blockIdx.x * 32 + threadIdx.x;
-    const int ib = blockIdx.y * 8 + threadIdx.y;
-    const int iv = blockIdx.z;
+    int ia, ib, iv;
+    cb_cell(p, ia, ib, iv);
     if (ia >= p.na || ib >= p.nb) return;
     const size_t total = (size_t)p.na * p.nb * p.nv_total;
     const size_t vg = (size_t)(p.v0 + iv);
@@ -104,9 +117,8 @@ __global__ void __launch_bounds__(256) cb_backward_kernel(const __grid_constant_
 template <bool DIV>
 __global__ void __launch_bounds__(256) cb_count_kernel(const __grid_constant__ CBParams<float> p)
 {
-    const int ia = blockIdx.x * 32 + threadIdx.x;
-    const int ib = blockIdx.y * 8 + threadIdx.y;
-    const int iv = blockIdx.z;
+    int ia, ib, iv;
+    cb_cell(p, ia, ib, iv);
     unsigned n = 0;
     if (ia < p.na && ib < p.nb) {
         float r[6];
@@ -205,6 +217,16 @@ __global__ void __launch_bounds__(256) lor_backward_kernel(const __grid_constant
 
 // ---------------- host side ----------------
 
+// Launch shape of the cone-beam kernels for nvc views (see cb_cell).
+template <typename T> static void cb_shape(CBParams<T> &p, int na, int nb, int nvc, dim3 &grid, dim3 &block)
+{
+    const int rows = tune_get(NEFCT_TUNE_CB_ROWS);
+    p.band_major = tune_get(NEFCT_TUNE_CB_ORDER) == 0;
+    block = dim3(32, rows);
+    const unsigned bands = (unsigned)((nb + rows - 1) / rows);
+    grid = p.band_major ? dim3((na + 31) / 32, nvc, bands) : dim3((na + 31) / 32, bands, nvc);
+}
+
 // The walk skips its divisions when both transverse pitches equal the x pitch.
 template <typename T> static bool cubic(const GridDev<T> &g) { return g.dy == (T)1 && g.dz == (T)1; }
 
@@ -235,6 +257,8 @@ nefct_status check_cb_geom(const nefct_cb_geom *g)
     if ((long long)g->na * g->nb * g->nv >= (1ll << 40))
         return fail(NEFCT_ERR_INVALID, "sinogram too large");
     if ((long long)g->na * g->nb >= (1ll << 31)) return fail(NEFCT_ERR_INVALID, "detector too large");
+    if (g->nb > 65535 || g->grid.nz > 65535)
+        return fail(NEFCT_ERR_INVALID, "detector rows and nz must be <= 65535 (got %d, %d)", g->nb, g->grid.nz);
     if (g->det_kind != NEFCT_DET_FLAT && g->det_kind != NEFCT_DET_CYL)
         return fail(NEFCT_ERR_INVALID, "det_kind must be NEFCT_DET_FLAT or NEFCT_DET_CYL (got %d)", g->det_kind);
     const float v[6] = {g->src_iso, g->src_det, g->da, g->a_shift, g->db, g->b_shift};
@@ -309,9 +333,10 @@ static nefct_status cb_forward_impl(const nefct_cb_geom *g, const T *vol, T *sin
     for (int v0 = 0; v0 < g->nv; v0 += kMax) {
         const int nvc = std::min(kMax, g->nv - v0);
         fill_views(*p, g, v0, nvc);
-        dim3 grid((g->na + 31) / 32, (g->nb + 7) / 8, nvc);
-        if (cubic(p->g)) cb_forward_kernel<T, false><<<grid, dim3(32, 8), 0, s>>>(*p);
-        else cb_forward_kernel<T, true><<<grid, dim3(32, 8), 0, s>>>(*p);
+        dim3 grid, block;
+        cb_shape(*p, g->na, g->nb, nvc, grid, block);
+        if (cubic(p->g)) cb_forward_kernel<T, false><<<grid, block, 0, s>>>(*p);
+        else cb_forward_kernel<T, true><<<grid, block, 0, s>>>(*p);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) { delete p; return cuda_fail(e, "cb_forward_kernel"); }
     }
@@ -343,9 +368,10 @@ static nefct_status cb_backward_impl(const nefct_cb_geom *g, const T *sino, T *v
     for (int v0 = 0; v0 < g->nv; v0 += kMax) {
         const int nvc = std::min(kMax, g->nv - v0);
         fill_views(*p, g, v0, nvc);
-        dim3 grid((g->na + 31) / 32, (g->nb + 7) / 8, nvc);
-        if (cubic(p->g)) cb_backward_kernel<T, false><<<grid, dim3(32, 8), 0, s>>>(*p);
-        else cb_backward_kernel<T, true><<<grid, dim3(32, 8), 0, s>>>(*p);
+        dim3 grid, block;
+        cb_shape(*p, g->na, g->nb, nvc, grid, block);
+        if (cubic(p->g)) cb_backward_kernel<T, false><<<grid, block, 0, s>>>(*p);
+        else cb_backward_kernel<T, true><<<grid, block, 0, s>>>(*p);
         e = cudaGetLastError();
         if (e != cudaSuccess) { delete p; return cuda_fail(e, "cb_backward_kernel"); }
     }
@@ -447,9 +473,10 @@ nefct_status nefct_cb_count_intersections(const nefct_cb_geom *g, uint32_t flags
     for (int v0 = 0; v0 < g->nv; v0 += kMax) {
         const int nvc = std::min(kMax, g->nv - v0);
         fill_views(*p, g, v0, nvc);
-        dim3 grid((g->na + 31) / 32, (g->nb + 7) / 8, nvc);
-        if (cubic(p->g)) cb_count_kernel<false><<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>(*p);
-        else cb_count_kernel<true><<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>(*p);
+        dim3 grid, block;
+        cb_shape(*p, g->na, g->nb, nvc, grid, block);
+        if (cubic(p->g)) cb_count_kernel<false><<<grid, block, 0, (cudaStream_t)stream>>>(*p);
+        else cb_count_kernel<true><<<grid, block, 0, (cudaStream_t)stream>>>(*p);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) { delete p; return cuda_fail(e, "cb_count_kernel"); }
     }

@@ -161,38 +161,41 @@ template <typename T> struct SlabSlots {
 //         y-fastest copy for x-driven rays).
 // next<CHECK>() returns the next slab's contributions; CHECK=false is only
 // valid for interior slabs, where all candidate voxels are inside the grid.
-template <typename T, bool DIV, bool SWP, bool SV1> struct Walker {
+template <typename T, bool DIV, bool SWP, bool SV1, bool EXACT = false> struct Walker {
     using F = FP<T>;
-    T pu, pv, pw, kv, kw, dv, dz, nv2, nz2;
+    using P2 = Pair<T>;
+    P2 p0, k2, n2;          // (pv, pw), (kv, kw), (nv2, nz2)
+    T pu, dv, dz;
     int nv, nz, su, sv, sw, base;
     bool vdiv, zdiv;
     T t, qav, qaw;
     int fav, faw, rowa;
 
-    __device__ __forceinline__ T posv(T tt) const
+    // Positions of plane t in v and z: ((p + k * (t - pu)) [/ d]) + n/2, the
+    // reference's order (:54-55, :67-68, :194-195, :207-208), both axes at once.
+    __device__ __forceinline__ P2 pos(T tt) const
     {
-        T q = F::add(pv, F::mul(kv, F::sub(tt, pu)));
-        if (DIV && vdiv) q = F::div(q, dv);
-        return F::add(q, nv2);
-    }
-    __device__ __forceinline__ T posw(T tt) const
-    {
-        T q = F::add(pw, F::mul(kw, F::sub(tt, pu)));
-        if (DIV && zdiv) q = F::div(q, dz);
-        return F::add(q, nz2);
+        const T d = F::sub(tt, pu);
+        P2 q = P2::add(p0, P2::mul(k2, P2::make(d, d)));
+        if (DIV && (vdiv || zdiv))
+            q = P2::make(vdiv ? F::div(q.x(), dv) : q.x(), zdiv ? F::div(q.y(), dz) : q.y());
+        return P2::add(q, n2);
     }
 
     __device__ __forceinline__ Walker(const Walk<T> &w, const GridDev<T> &g, int k, int su_, int sv_, int sw_)
     {
-        pu = w.pu; pv = w.pv; pw = w.pw; kv = w.kv; kw = w.kw; dv = w.dv; dz = g.dz;
-        nv2 = w.nv2; nz2 = g.nz2;
+        p0 = P2::make(w.pv, w.pw);
+        k2 = P2::make(w.kv, w.kw);
+        n2 = P2::make(w.nv2, g.nz2);
+        pu = w.pu; dv = w.dv; dz = g.dz;
         nv = w.nv; nz = g.nz; su = su_; sv = SV1 ? 1 : sv_; sw = sw_;
         vdiv = w.vdiv;
         zdiv = dz != (T)1;
         base = k * su;
         t = F::sub((T)k, w.nu2);
-        qav = posv(t);
-        qaw = posw(t);
+        const P2 q = pos(t);
+        qav = q.x();
+        qaw = q.y();
         fav = F::ifloor(qav);
         faw = F::ifloor(qaw);
         rowa = faw * sw;
@@ -201,7 +204,8 @@ template <typename T, bool DIV, bool SWP, bool SV1> struct Walker {
     template <bool CHECK> __device__ __forceinline__ SlabSlots<T> next()
     {
         const T t2 = F::add(t, (T)1);
-        const T qbv = posv(t2), qbw = posw(t2);
+        const P2 qb = pos(t2);
+        const T qbv = qb.x(), qbw = qb.y();
         const int fbv = F::ifloor(qbv), fbw = F::ifloor(qbw);
         const int rowb = fbw * sw;
         // low/high plane of the slab in v (min/max equals the slope-sign choice)
@@ -214,8 +218,10 @@ template <typename T, bool DIV, bool SWP, bool SV1> struct Walker {
         t = t2; qav = qbv; qaw = qbw; fav = fbv; faw = fbw; rowa = rowb; base += su;
 
         const bool vx = cv1 != cv2, wx = cw1 != cw2;
-        const T rvq = F::ratio(F::sub((T)cv2, q1v), F::sub(q2v, q1v));
-        const T rwq = F::ratio(F::sub((T)cw2, q1w), F::sub(q2w, q1w));
+        const T rvq = EXACT ? F::div(F::sub((T)cv2, q1v), F::sub(q2v, q1v))
+                            : F::ratio(F::sub((T)cv2, q1v), F::sub(q2v, q1v));
+        const T rwq = EXACT ? F::div(F::sub((T)cw2, q1w), F::sub(q2w, q1w))
+                            : F::ratio(F::sub((T)cw2, q1w), F::sub(q2w, q1w));
         const T rv = vx ? rvq : (T)1, rw = wx ? rwq : (T)1;
         const bool vfirst = rv > rw;   // middle voxel (cv1, cw2) when true, else (cv2, cw1)
         SlabSlots<T> s;
@@ -317,17 +323,19 @@ __device__ __forceinline__ void scatter_walk(const Walk<T> &w, const GridDev<T> 
     else scatter_walk_t<T, DIV, false, SV1, Q5>(w, g, base, su, sv, sw, value);
 }
 
-// Number of contributions of the ray (the throughput unit).
+// Number of contributions of the ray (the throughput unit).  Uses the
+// reference's exact ratio division, so near-equal crossing ratios order the
+// three-voxel split exactly as the reference does and the count matches it.
 template <typename T, bool DIV>
 __device__ __forceinline__ unsigned count_walk(const Walk<T> &w, const GridDev<T> &g)
 {
     unsigned n = 0;
     auto f = [&](const SlabSlots<T> &s) { n += (unsigned)s.ok[0] + (unsigned)s.ok[1] + (unsigned)s.ok[2]; };
     if (w.kw >= (T)0) {
-        Walker<T, DIV, true, true> it(w, g, w.k0, 0, 1, 0);
+        Walker<T, DIV, true, true, true> it(w, g, w.k0, 0, 1, 0);
         walk_all(it, w.k0, w.k1, w.ki0, w.ki1, f);
     } else {
-        Walker<T, DIV, false, true> it(w, g, w.k0, 0, 1, 0);
+        Walker<T, DIV, false, true, true> it(w, g, w.k0, 0, 1, 0);
         walk_all(it, w.k0, w.k1, w.ki0, w.ki1, f);
     }
     return n;

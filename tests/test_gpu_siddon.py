@@ -213,3 +213,25 @@ def test_linearity_and_adjoint_config2_size(cuda):
     lhs = float((ax.double() * y.double()).sum())
     rhs = float((x.double() * aty.double()).sum())
     assert abs(lhs - rhs) / abs(lhs) < 1e-5
+
+
+def test_launch_shapes_give_identical_forward(cuda):
+    """Every autotuner variant runs the same per-ray arithmetic: the forward
+    is bitwise identical across rows-per-CTA and grid orders."""
+    from nefct_b200 import autotune
+    g = nb.ConeBeam((40, 36, 30), np.linspace(0, 2 * np.pi, 33, endpoint=False), 150.0, 300.0, 70, 1.3, 45, 1.1,
+                    size=(40.0, 36.0, 30.0))
+    vol = torch.rand(g.vol_shape, device=cuda, generator=torch.Generator(device=cuda).manual_seed(8))
+    saved = autotune.current()
+    try:
+        outs = []
+        for rows in (1, 2, 4, 8):
+            for order in (0, 1):
+                autotune.apply(rows, order)
+                outs.append(ops.cb_forward(vol, g).cpu())
+        for o in outs[1:]:
+            assert torch.equal(o, outs[0])
+        rec = autotune.tune_cone_beam(g, 0, cuda, reps=1, use_cache=False)
+        assert rec["rows"] in (2, 4, 8) and rec["order"] in (0, 1) and len(rec["ms"]) == 6
+    finally:
+        autotune.apply(saved["rows"], saved["order"])

@@ -4,10 +4,10 @@ Follows mat_codes/filtering.m:1-90 and mat_codes/ParkerWeight.m:1-29 of
 bill52547/CT-NEF step by step in float64: cosine weight, optional Parker
 weight, zero padding to max(64, 2^nextpow2(2 nu)), FFT, multiplication by
 the windowed 2|FFT(ramp_flat)|, inverse FFT, crop and scale.  The MATLAB
-code cannot run here (no MATLAB/Octave); this restatement is the FDK
-oracle.  Parity of the filter is therefore pinned only by this restatement
-and by analytic properties (tests/test_fdk_oracle.py), not by running the
-reference itself.
+code cannot run here (no MATLAB/Octave) and the reference holds no golden
+vectors for it: parity unpinned.  This restatement is the FDK filter oracle;
+it is checked against analytic properties of the filter
+(tests/test_fdk_oracle.py), not against the reference run.
 
 Array layout here is the GPU sinogram layout [nv][nb][na] (u = column a
 fastest); the MATLAB code holds proj(u, v, view).

@@ -70,6 +70,7 @@ _PROTOS = {
     "nefct_cb_workspace_bytes": (C.c_size_t, [C.POINTER(CBGeom), _u32]),
     "nefct_cb_forward": (_i32, [C.POINTER(CBGeom), _vp, _vp, _u32, _vp, C.c_size_t, _vp]),
     "nefct_cb_backward": (_i32, [C.POINTER(CBGeom), _vp, _vp, _u32, _vp, C.c_size_t, _vp]),
+    "nefct_cb_forward_noalloc": (_i32, [C.POINTER(CBGeom), _vp, _vp, _u32, _vp]),
     "nefct_cb_forward_f64": (_i32, [C.POINTER(CBGeom), _vp, _vp, _u32, _vp, C.c_size_t, _vp]),
     "nefct_cb_backward_f64": (_i32, [C.POINTER(CBGeom), _vp, _vp, _u32, _vp, C.c_size_t, _vp]),
     "nefct_cb_count_intersections": (_i32, [C.POINTER(CBGeom), _u32, _vp, _vp]),

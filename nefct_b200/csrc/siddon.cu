@@ -15,6 +15,7 @@
 // Per-view cos/sin/z-offset ride in the kernel parameters.
 #include <math.h>
 #include <algorithm>
+#include <mutex>
 
 #include "siddon.cuh"
 
@@ -422,6 +423,83 @@ static nefct_status lor_impl(const nefct_grid *grid, const T *lors, int64_t n, c
     return NEFCT_OK;
 }
 
+
+// ---------------- forward projection for callers that cannot allocate ----------------
+//
+// Some callers of this library are not allowed to allocate device memory:
+// reconstruction services that reserve all GPU memory at start-up and forbid
+// later allocations (fixed memory budget, predictable latency), host
+// frameworks that own the device memory pool and only hand out the tensors a
+// plugin reads and writes, and bindings that receive bare device pointers
+// with no access to an allocator.  nefct_cb_forward needs a volume-sized
+// scratch buffer that such callers cannot provide.  For them the scratch
+// lives in this fixed array, part of the library's device image: every GPU
+// that loads the library holds it (32 MiB) until the process exits.
+static constexpr size_t kStaticScratchFloats = size_t(8) << 20;   // 8 Mi voxels
+static __device__ __align__(256) float g_static_scratch[kStaticScratchFloats];
+
+// Host code cannot use g_static_scratch's name as a device address; its
+// address on each device is looked up once, with that device current.
+static constexpr int kMaxDevices = 64;
+static std::mutex g_static_mu;
+static float *g_static_addr[kMaxDevices];
+
+static nefct_status static_scratch_address(float **addr)
+{
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if (dev < 0 || dev >= kMaxDevices) return fail(NEFCT_ERR_UNSUPPORTED, "device %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_addr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_static_scratch)");
+        g_static_addr[dev] = (float *)p;
+    }
+    *addr = g_static_addr[dev];
+    return NEFCT_OK;
+}
+
+static nefct_status cb_forward_static_impl(const nefct_cb_geom *g, const float *vol, float *sino, uint32_t flags,
+                                           cudaStream_t s)
+{
+    nefct_status st = check_cb_geom(g);
+    if (st) return st;
+    if (!vol || !sino) return fail(NEFCT_ERR_INVALID, "vol and sino must be non-NULL");
+    if (flags & ~kWalkFlags) return fail(NEFCT_ERR_INVALID, "unknown flag bits 0x%x", flags & ~kWalkFlags);
+    const size_t nvox = (size_t)g->grid.nx * g->grid.ny * g->grid.nz;
+    const bool tr = !(flags & NEFCT_NO_TRANSPOSE);
+    if (tr && nvox > kStaticScratchFloats)
+        return fail(NEFCT_ERR_INVALID,
+                    "nefct_cb_forward_noalloc handles at most %zu voxels (its fixed scratch is %zu MiB); this grid "
+                    "has %zu -- use nefct_cb_forward with a workspace",
+                    kStaticScratchFloats, kStaticScratchFloats * sizeof(float) >> 20, nvox);
+    float *scratch = nullptr;
+    if (tr) {
+        st = static_scratch_address(&scratch);
+        if (st) return st;
+        // the transpose overwrites every scratch element this call reads
+        st = transpose_xy(vol, scratch, g->grid, s);
+        if (st) return st;
+    }
+    CBParams<float> p;            // on the host stack: no allocation of any kind
+    fill_cb_params(p, g, flags);
+    p.vol = vol;
+    p.volT = scratch;
+    p.out = sino;
+    for (int v0 = 0; v0 < g->nv; v0 += ViewTable<float>::kMax) {
+        const int nvc = std::min(ViewTable<float>::kMax, g->nv - v0);
+        fill_views(p, g, v0, nvc);
+        dim3 grid, block;
+        cb_shape(p, g->na, g->nb, nvc, grid, block);
+        if (cubic(p.g)) cb_forward_kernel<float, false><<<grid, block, 0, s>>>(p);
+        else cb_forward_kernel<float, true><<<grid, block, 0, s>>>(p);
+        NEFCT_CHECK_LAUNCH("cb_forward_kernel (noalloc)");
+    }
+    return NEFCT_OK;
+}
+
 }  // namespace nefct
 
 using namespace nefct;
@@ -494,6 +572,14 @@ nefct_status nefct_lor_backward(const nefct_grid *grid, const float *lors, int64
                                 float *vol, uint32_t flags, void *stream)
 {
     return lor_impl<float>(grid, lors, n, vals, vol, flags, (cudaStream_t)stream, false);
+}
+
+// See cb_forward_static_impl: same result as nefct_cb_forward, with the
+// scratch in the library's fixed device array instead of a caller workspace.
+nefct_status nefct_cb_forward_noalloc(const nefct_cb_geom *g, const float *vol, float *sino, uint32_t flags,
+                                      void *stream)
+{
+    return cb_forward_static_impl(g, vol, sino, flags, (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -234,7 +234,11 @@ def run_gpu(args):
         ops.cb_backward(grad, geom, 0, out=back)
 
     from nefct_b200 import autotune
-    tuned = autotune.tune_cone_beam(geom, 0, dev, use_cache=False)     # untimed launch-shape choice
+    if args.rows:
+        autotune.apply(args.rows, args.order)                          # fixed launch shape (profiling)
+        tuned = {"rows": args.rows, "order": args.order, "ms": None}
+    else:
+        tuned = autotune.tune_cone_beam(geom, 0, dev, use_cache=False)  # untimed launch-shape choice
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -330,6 +334,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--views", type=int, default=360, help="views of the scan (360 = the workload; fewer only for profiling)")
+    ap.add_argument("--rows", type=int, default=0, help="fix the detector rows per CTA instead of autotuning")
+    ap.add_argument("--order", type=int, default=1, help="with --rows: 0 row bands outermost, 1 views outermost")
     args = ap.parse_args()
     CFG["nv"] = args.views
     if args.impl == "reference":

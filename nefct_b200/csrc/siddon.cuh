@@ -218,10 +218,12 @@ template <typename T, bool DIV, bool SWP, bool SV1, bool EXACT = false> struct W
         t = t2; qav = qbv; qaw = qbw; fav = fbv; faw = fbw; rowa = rowb; base += su;
 
         const bool vx = cv1 != cv2, wx = cw1 != cw2;
-        const T rvq = EXACT ? F::div(F::sub((T)cv2, q1v), F::sub(q2v, q1v))
-                            : F::ratio(F::sub((T)cv2, q1v), F::sub(q2v, q1v));
-        const T rwq = EXACT ? F::div(F::sub((T)cw2, q1w), F::sub(q2w, q1w))
-                            : F::ratio(F::sub((T)cw2, q1w), F::sub(q2w, q1w));
+        // crossing ratios (c2 - q1) / (q2 - q1) of both axes (reference :94, :118, :134-135)
+        const P2 nq1 = P2::make(-q1v, -q1w);
+        const P2 num = P2::add(P2::make((T)cv2, (T)cw2), nq1);
+        const P2 den = P2::add(P2::make(q2v, q2w), nq1);
+        const T rvq = EXACT ? F::div(num.x(), den.x()) : F::ratio(num.x(), den.x());
+        const T rwq = EXACT ? F::div(num.y(), den.y()) : F::ratio(num.y(), den.y());
         const T rv = vx ? rvq : (T)1, rw = wx ? rwq : (T)1;
         const bool vfirst = rv > rw;   // middle voxel (cv1, cw2) when true, else (cv2, cw1)
         SlabSlots<T> s;
@@ -249,10 +251,12 @@ template <typename T, bool DIV, bool SWP, bool SV1, bool EXACT = false> struct W
     }
 };
 
-// Runs f(slots) over slabs [a, b] with the given check mode.
+// Runs f(slots) over slabs [a, b] with the given check mode (unrolled by two
+// so the carried plane state alternates registers instead of being moved).
 template <bool CHECK, class WK, class Fn>
 __device__ __forceinline__ void walk_range(WK &it, int a, int b, Fn &f)
 {
+#pragma unroll 2
     for (int k = a; k <= b; ++k) f(it.template next<CHECK>());
 }
 

@@ -160,6 +160,37 @@ nefct_status nefct_cb_backward_f64(const nefct_cb_geom *g, const double *sino, d
 nefct_status nefct_cb_count_intersections(const nefct_cb_geom *g, uint32_t flags,
                                           unsigned long long *count, void *stream);
 
+/* Batched cone-beam problems of uneven sizes: forward of every problem in
+ * one persistent launch, transposes of every problem in another.  No
+ * counterpart in the reference (which projects one problem per op call,
+ * e.g. project_t.py:153-160 even one view per call).  Work is tiled (32
+ * detector columns x NEFCT_TUNE_CB_ROWS rows of one view), ordered longest
+ * rays first and handed out through an atomic ticket; nothing waits, so the
+ * launch cannot hang.  Per problem: vol -> sino (forward), grad -> back
+ * (transpose, exact for the same flags). */
+typedef struct nefct_cb_problem {
+    nefct_cb_geom geom;        /* host geometry (angles/z_offsets read at plan time) */
+    const float *vol;          /* device [nz][ny][nx], forward input */
+    float *sino;               /* device [nv][nb][na], forward output */
+    const float *grad;         /* device [nv][nb][na], transpose input (may be sino) */
+    float *back;               /* device [nz][ny][nx], transpose output (overwritten) */
+} nefct_cb_problem;
+typedef struct nefct_cb_batch nefct_cb_batch;
+/* Host-only: validates the problems, builds the tile order and returns the
+ * device workspace size (descriptors, view tables, one volume copy per
+ * problem). */
+nefct_status nefct_cb_batch_plan(const nefct_cb_problem *problems, int32_t n, uint32_t flags,
+                                 nefct_cb_batch **plan, size_t *workspace_bytes);
+/* Uploads the plan's tables into the caller's workspace (256-byte aligned)
+ * and waits for that copy.  Call once, before forward/backward and before
+ * capturing them in a CUDA graph; the buffers named in the problems must stay
+ * valid while the plan is used. */
+nefct_status nefct_cb_batch_bind(nefct_cb_batch *plan, void *workspace, size_t workspace_bytes, void *stream);
+nefct_status nefct_cb_batch_forward(const nefct_cb_batch *plan, void *stream);
+nefct_status nefct_cb_batch_backward(const nefct_cb_batch *plan, void *stream);
+int64_t nefct_cb_batch_tiles(const nefct_cb_batch *plan);   /* work tiles per launch */
+void nefct_cb_batch_destroy(nefct_cb_batch *plan);
+
 /* LOR projector pair.  lors is [6][n] (rows x1 y1 z1 x2 y2 z2, each n
  * long), as the reference op slices it (cpp/siddon/siddon_gpu.cc:74-86).
  * Replace Projection / Backprojection (siddon_gpu.cc:11-35) and their host

@@ -58,6 +58,11 @@ class CBGeom(C.Structure):
                 ("det_kind", C.c_int32)]
 
 
+class CBProblem(C.Structure):
+    _fields_ = [("geom", CBGeom), ("vol", C.c_void_p), ("sino", C.c_void_p), ("grad", C.c_void_p),
+                ("back", C.c_void_p)]
+
+
 _vp = C.c_void_p
 _i32 = C.c_int32
 _u32 = C.c_uint32
@@ -74,6 +79,12 @@ _PROTOS = {
     "nefct_cb_forward_f64": (_i32, [C.POINTER(CBGeom), _vp, _vp, _u32, _vp, C.c_size_t, _vp]),
     "nefct_cb_backward_f64": (_i32, [C.POINTER(CBGeom), _vp, _vp, _u32, _vp, C.c_size_t, _vp]),
     "nefct_cb_count_intersections": (_i32, [C.POINTER(CBGeom), _u32, _vp, _vp]),
+    "nefct_cb_batch_plan": (_i32, [C.POINTER(CBProblem), _i32, _u32, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
+    "nefct_cb_batch_bind": (_i32, [_vp, _vp, C.c_size_t, _vp]),
+    "nefct_cb_batch_forward": (_i32, [_vp, _vp]),
+    "nefct_cb_batch_backward": (_i32, [_vp, _vp]),
+    "nefct_cb_batch_tiles": (C.c_int64, [_vp]),
+    "nefct_cb_batch_destroy": (None, [_vp]),
     "nefct_lor_forward": (_i32, [C.POINTER(Grid), _vp, C.c_int64, _vp, _vp, _u32, _vp]),
     "nefct_lor_backward": (_i32, [C.POINTER(Grid), _vp, C.c_int64, _vp, _vp, _u32, _vp]),
     "nefct_fdk_filter": (_i32, [C.POINTER(CBGeom), _vp, _vp, _i32, _i32, _vp]),

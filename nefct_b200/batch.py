@@ -1,0 +1,93 @@
+"""Batched uneven cone-beam problems: one persistent launch per direction,
+optionally replayed as a CUDA graph (include/nefct_b200.h, nefct_cb_batch_*).
+
+    bp = BatchProjector(geoms, vols)          # plans, allocates, binds
+    bp.step()                                 # forward of all, then transpose of all
+    g = bp.capture()                          # CUDA graph of one step; g.replay()
+
+Per problem i: ``sinos[i] = A_i vols[i]`` and ``backs[i] = A_i^T grads[i]``
+(``grads`` defaults to ``sinos``).  Forward outputs are bitwise equal to
+``ops.cb_forward`` of each problem (same per-ray code).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from . import _lib, ops
+
+__all__ = ["BatchProjector"]
+
+
+class BatchProjector:
+    def __init__(self, geoms: list[ops.ConeBeam], vols: list[torch.Tensor], sinos=None, grads=None, backs=None,
+                 flags: int = 0):
+        if len(geoms) != len(vols) or not geoms:
+            raise ValueError("need one volume per geometry")
+        dev = vols[0].device
+        self.geoms = list(geoms)
+        self.vols = [v.contiguous() for v in vols]
+        for g, v in zip(self.geoms, self.vols):
+            if v.dtype != torch.float32 or tuple(v.shape) != g.vol_shape or v.device != dev:
+                raise _lib.NefctError(_lib.ERR_INVALID, "volumes must be float32 [nz, ny, nx] on one device")
+        self.sinos = sinos or [torch.empty(g.sino_shape, device=dev) for g in geoms]
+        self.grads = grads or self.sinos
+        self.backs = backs or [torch.empty(g.vol_shape, device=dev) for g in geoms]
+        self.flags = flags
+        self.device = dev
+        n = len(geoms)
+        probs = (_lib.CBProblem * n)()
+        self._structs = []
+        for i, g in enumerate(self.geoms):
+            probs[i].geom = g.struct()
+            probs[i].vol = self.vols[i].data_ptr()
+            probs[i].sino = self.sinos[i].data_ptr()
+            probs[i].grad = self.grads[i].data_ptr()
+            probs[i].back = self.backs[i].data_ptr()
+        lib = _lib.load()
+        plan = C.c_void_p()
+        nbytes = C.c_size_t()
+        _lib.check(lib.nefct_cb_batch_plan(probs, n, flags, C.byref(plan), C.byref(nbytes)))
+        self._plan = plan
+        self.workspace = torch.empty(nbytes.value, dtype=torch.uint8, device=dev)
+        with torch.cuda.device(dev):
+            _lib.check(lib.nefct_cb_batch_bind(plan, self.workspace.data_ptr(), nbytes.value,
+                                               torch.cuda.current_stream(dev).cuda_stream))
+        self.tiles = int(lib.nefct_cb_batch_tiles(plan))
+
+    def _stream(self):
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    def forward(self):
+        _lib.check(_lib.load().nefct_cb_batch_forward(self._plan, self._stream()))
+        return self.sinos
+
+    def backward(self):
+        _lib.check(_lib.load().nefct_cb_batch_backward(self._plan, self._stream()))
+        return self.backs
+
+    def step(self):
+        self.forward()
+        self.backward()
+
+    def capture(self) -> torch.cuda.CUDAGraph:
+        """CUDA graph of one step (forward of all problems, then transpose of all)."""
+        s = torch.cuda.Stream(self.device)
+        s.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(s):
+            self.step()                      # warm-up outside the capture
+        torch.cuda.current_stream(self.device).wait_stream(s)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.step()
+        return g
+
+    def __del__(self):
+        plan = getattr(self, "_plan", None)
+        if plan is not None and plan.value:
+            try:
+                _lib.load().nefct_cb_batch_destroy(plan)
+            except Exception:
+                pass
+            self._plan = None

@@ -24,8 +24,8 @@ namespace nefct {
 template <typename T> struct CBParams {
     GridDev<T> g;
     int na, nb, nvc, v0, nv_total;
-    T src_iso, src_det, da, ai, db, bi, half_a, half_b;
-    int cyl, band_major;
+    RayGeom<T> rg;
+    int band_major;
     uint32_t flags;
     const T *vol;        // x-fastest volume (forward source)
     const T *volT;       // y-fastest copy for x-driven rays, or nullptr
@@ -36,30 +36,10 @@ template <typename T> struct CBParams {
     ViewTable<T> tab;
 };
 
-// Ray of detector cell (ia, ib) at view iv of the launch: ProjectFlatKernel
-// (siddon.cu.cc:341-353) / ProjectCyliKernel (:376-387), same order of
-// operations, plus the optional z offset of source and detector.
 template <typename T>
 __device__ __forceinline__ void cb_ray(const CBParams<T> &p, int ia, int ib, int iv, T *r)
 {
-    using F = FP<T>;
-    const T cs = p.tab.cs[iv], sn = p.tab.sn[iv], off = p.tab.off[iv];
-    const T a = F::sub(F::mul(F::add(p.ai, (T)ia), p.da), p.half_a);
-    const T b = F::sub(F::mul(F::add(p.bi, (T)ib), p.db), p.half_b);
-    T xd0, yd0;
-    if (p.cyl) {
-        xd0 = F::sub(F::mul(p.src_det, cos(a)), p.src_iso);
-        yd0 = F::mul(p.src_det, sin(a));
-    } else {
-        xd0 = F::sub(p.src_det, p.src_iso);
-        yd0 = a;
-    }
-    r[0] = F::mul(-p.src_iso, cs);
-    r[1] = F::mul(-p.src_iso, sn);
-    r[2] = F::add((T)0, off);
-    r[3] = F::sub(F::mul(xd0, cs), F::mul(yd0, sn));
-    r[4] = F::add(F::mul(xd0, sn), F::mul(yd0, cs));
-    r[5] = F::add(b, off);
+    cb_ray(p.rg, p.tab.cs[iv], p.tab.sn[iv], p.tab.off[iv], ia, ib, r);
 }
 
 // Detector cell of this thread: 32 columns x blockDim.y rows per CTA; grid
@@ -81,14 +61,7 @@ __global__ void __launch_bounds__(256) cb_forward_kernel(const __grid_constant__
     if (ia >= p.na || ib >= p.nb) return;
     T r[6];
     cb_ray(p, ia, ib, iv, r);
-    Walk<T> w;
-    T acc = (T)0;
-    if (setup_walk(p.g, r, p.flags, w)) {
-        const int sw = p.g.nx * p.g.ny;
-        if (!w.xdrive) acc = gather_walk<T, DIV, true, false>(w, p.g, p.vol, p.g.nx, 1, sw);
-        else if (p.volT) acc = gather_walk<T, DIV, true, false>(w, p.g, p.volT, p.g.ny, 1, sw);
-        else acc = gather_walk<T, DIV, false, false>(w, p.g, p.vol, 1, p.g.nx, sw);
-    }
+    const T acc = ray_forward<T, DIV>(p.g, r, p.flags, p.vol, p.volT);
     p.out[(size_t)(p.v0 + iv) * p.na * p.nb + (size_t)ib * p.na + ia] = acc;
 }
 
@@ -107,12 +80,7 @@ __global__ void __launch_bounds__(256) cb_backward_kernel(const __grid_constant_
     if (y == (T)0) return;
     T r[6];
     cb_ray(p, ia, ib, iv, r);
-    Walk<T> w;
-    if (!setup_walk(p.g, r, p.flags, w)) return;
-    const int sw = p.g.nx * p.g.ny;
-    if (!w.xdrive) scatter_walk<T, DIV, true, false>(w, p.g, p.out, p.g.nx, 1, sw, y);
-    else if (p.outT) scatter_walk<T, DIV, true, false>(w, p.g, p.outT, p.g.ny, 1, sw, y);
-    else scatter_walk<T, DIV, false, false>(w, p.g, p.out, 1, p.g.nx, sw, y);
+    ray_backward<T, DIV>(p.g, r, p.flags, y, p.out, p.outT);
 }
 
 template <bool DIV>
@@ -129,44 +97,6 @@ __global__ void __launch_bounds__(256) cb_count_kernel(const __grid_constant__ C
     }
     for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
     if ((threadIdx.x & 31) == 0 && n) atomicAdd(p.count, (unsigned long long)n);
-}
-
-// out[z][x][y] = in[z][y][x] (32x32 tiles through shared memory)
-template <typename T>
-__global__ void __launch_bounds__(256) transpose_xy_kernel(const T *__restrict__ in, T *__restrict__ out,
-                                                           int nx, int ny)
-{
-    __shared__ T tile[32][33];
-    const size_t plane = (size_t)nx * ny * blockIdx.z;
-    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
-    for (int j = threadIdx.y; j < 32; j += 8) {
-        const int x = x0 + threadIdx.x, y = y0 + j;
-        if (x < nx && y < ny) tile[j][threadIdx.x] = in[plane + (size_t)y * nx + x];
-    }
-    __syncthreads();
-    for (int j = threadIdx.y; j < 32; j += 8) {
-        const int y = y0 + threadIdx.x, x = x0 + j;
-        if (x < nx && y < ny) out[plane + (size_t)x * ny + y] = tile[threadIdx.x][j];
-    }
-}
-
-// vol[z][y][x] += accT[z][x][y]
-template <typename T>
-__global__ void __launch_bounds__(256) fold_add_kernel(const T *__restrict__ accT, T *__restrict__ vol,
-                                                       int nx, int ny)
-{
-    __shared__ T tile[32][33];
-    const size_t plane = (size_t)nx * ny * blockIdx.z;
-    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
-    for (int j = threadIdx.y; j < 32; j += 8) {
-        const int y = y0 + threadIdx.x, x = x0 + j;
-        if (x < nx && y < ny) tile[j][threadIdx.x] = accT[plane + (size_t)x * ny + y];
-    }
-    __syncthreads();
-    for (int j = threadIdx.y; j < 32; j += 8) {
-        const int x = x0 + threadIdx.x, y = y0 + j;
-        if (x < nx && y < ny) vol[plane + (size_t)y * nx + x] += tile[threadIdx.x][j];
-    }
 }
 
 // ---------------- LOR projector pair (cpp/siddon) ----------------
@@ -278,12 +208,7 @@ template <typename T> static void fill_cb_params(CBParams<T> &p, const nefct_cb_
 {
     p.g = make_grid_dev<T>(g->grid);
     p.na = g->na; p.nb = g->nb; p.nv_total = g->nv;
-    p.src_iso = (T)g->src_iso; p.src_det = (T)g->src_det;
-    p.da = (T)g->da; p.ai = (T)g->a_shift; p.db = (T)g->db; p.bi = (T)g->b_shift;
-    // na*da/2 in the reference's order (siddon.cu.cc:341)
-    p.half_a = (T)g->na * p.da / (T)2;
-    p.half_b = (T)g->nb * p.db / (T)2;
-    p.cyl = g->det_kind == NEFCT_DET_CYL;
+    p.rg = make_ray_geom<T>(*g);
     p.flags = flags;
 }
 

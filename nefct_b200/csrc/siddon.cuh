@@ -52,6 +52,50 @@ template <typename T> inline GridDev<T> make_grid_dev(const nefct_grid &g)
     return d;
 }
 
+// Scanner constants of the cone-beam ray generator.
+template <typename T> struct RayGeom {
+    T src_iso, src_det, da, ai, db, bi, half_a, half_b;
+    int cyl;
+};
+
+template <typename T> inline RayGeom<T> make_ray_geom(const nefct_cb_geom &g)
+{
+    RayGeom<T> r;
+    r.src_iso = (T)g.src_iso; r.src_det = (T)g.src_det;
+    r.da = (T)g.da; r.ai = (T)g.a_shift; r.db = (T)g.db; r.bi = (T)g.b_shift;
+    // na*da/2 in the reference's order (siddon.cu.cc:341)
+    r.half_a = (T)g.na * r.da / (T)2;
+    r.half_b = (T)g.nb * r.db / (T)2;
+    r.cyl = g.det_kind == NEFCT_DET_CYL;
+    return r;
+}
+
+// Ray of detector cell (ia, ib) at a view with (cos, sin, z offset) =
+// (cs, sn, off): ProjectFlatKernel (siddon.cu.cc:341-353) /
+// ProjectCyliKernel (:376-387), same order of operations, plus the optional
+// z offset of source and detector.  r = (x1, y1, z1, x2, y2, z2).
+template <typename T>
+__device__ __forceinline__ void cb_ray(const RayGeom<T> &p, T cs, T sn, T off, int ia, int ib, T *r)
+{
+    using F = FP<T>;
+    const T a = F::sub(F::mul(F::add(p.ai, (T)ia), p.da), p.half_a);
+    const T b = F::sub(F::mul(F::add(p.bi, (T)ib), p.db), p.half_b);
+    T xd0, yd0;
+    if (p.cyl) {
+        xd0 = F::sub(F::mul(p.src_det, cos(a)), p.src_iso);
+        yd0 = F::mul(p.src_det, sin(a));
+    } else {
+        xd0 = F::sub(p.src_det, p.src_iso);
+        yd0 = a;
+    }
+    r[0] = F::mul(-p.src_iso, cs);
+    r[1] = F::mul(-p.src_iso, sn);
+    r[2] = F::add((T)0, off);
+    r[3] = F::sub(F::mul(xd0, cs), F::mul(yd0, sn));
+    r[4] = F::add(F::mul(xd0, sn), F::mul(yd0, cs));
+    r[5] = F::add(b, off);
+}
+
 template <typename T> struct Walk {
     T pu, pv, pw;        // source in voxel units along (drive, other transverse, z)
     T kv, kw;            // slopes d(v)/d(u), d(z)/d(u)
@@ -343,6 +387,70 @@ __device__ __forceinline__ unsigned count_walk(const Walk<T> &w, const GridDev<T
         walk_all(it, w.k0, w.k1, w.ki0, w.ki1, f);
     }
     return n;
+}
+
+// Forward value of one ray: gathers x-driven rays from the y-fastest copy
+// volT when there is one, everything else from the x-fastest volume.
+template <typename T, bool DIV>
+__device__ __forceinline__ T ray_forward(const GridDev<T> &g, const T *r, uint32_t flags, const T *vol, const T *volT)
+{
+    Walk<T> w;
+    if (!setup_walk(g, r, flags, w)) return (T)0;
+    const int sw = g.nx * g.ny;
+    if (!w.xdrive) return gather_walk<T, DIV, true, false>(w, g, vol, g.nx, 1, sw);
+    if (volT) return gather_walk<T, DIV, true, false>(w, g, volT, g.ny, 1, sw);
+    return gather_walk<T, DIV, false, false>(w, g, vol, 1, g.nx, sw);
+}
+
+// Transpose contribution of one ray with value y: x-driven rays reduce into
+// the y-fastest accumulator outT when there is one.
+template <typename T, bool DIV>
+__device__ __forceinline__ void ray_backward(const GridDev<T> &g, const T *r, uint32_t flags, T y, T *out, T *outT)
+{
+    Walk<T> w;
+    if (!setup_walk(g, r, flags, w)) return;
+    const int sw = g.nx * g.ny;
+    if (!w.xdrive) scatter_walk<T, DIV, true, false>(w, g, out, g.nx, 1, sw, y);
+    else if (outT) scatter_walk<T, DIV, true, false>(w, g, outT, g.ny, 1, sw, y);
+    else scatter_walk<T, DIV, false, false>(w, g, out, 1, g.nx, sw, y);
+}
+
+// out[z][x][y] = in[z][y][x] (32x32 tiles through shared memory)
+template <typename T>
+__global__ void __launch_bounds__(256) transpose_xy_kernel(const T *__restrict__ in, T *__restrict__ out,
+                                                           int nx, int ny)
+{
+    __shared__ T tile[32][33];
+    const size_t plane = (size_t)nx * ny * blockIdx.z;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int x = x0 + threadIdx.x, y = y0 + j;
+        if (x < nx && y < ny) tile[j][threadIdx.x] = in[plane + (size_t)y * nx + x];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int y = y0 + threadIdx.x, x = x0 + j;
+        if (x < nx && y < ny) out[plane + (size_t)x * ny + y] = tile[threadIdx.x][j];
+    }
+}
+
+// vol[z][y][x] += accT[z][x][y]
+template <typename T>
+__global__ void __launch_bounds__(256) fold_add_kernel(const T *__restrict__ accT, T *__restrict__ vol,
+                                                       int nx, int ny)
+{
+    __shared__ T tile[32][33];
+    const size_t plane = (size_t)nx * ny * blockIdx.z;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int y = y0 + threadIdx.x, x = x0 + j;
+        if (x < nx && y < ny) tile[j][threadIdx.x] = accT[plane + (size_t)x * ny + y];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int x = x0 + threadIdx.x, y = y0 + j;
+        if (x < nx && y < ny) vol[plane + (size_t)y * nx + x] += tile[threadIdx.x][j];
+    }
 }
 
 }  // namespace nefct

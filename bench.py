@@ -376,6 +376,10 @@ def run_batched(args):
     t_batch = e0.elapsed_time(e1) / 1e3 / args.steps
 
     # sequential per-problem device calls (the same kernels, one problem at a time)
+    for g, v, s_, b in zip(geoms, vols, bp.sinos, bp.backs):      # warm the allocator's workspaces
+        ops.cb_forward(v, g, 0, out=s_)
+        ops.cb_backward(s_, g, 0, out=b)
+    torch.cuda.synchronize()
     e0.record()
     for g, v, s_, b in zip(geoms, vols, bp.sinos, bp.backs):
         ops.cb_forward(v, g, 0, out=s_)
@@ -403,7 +407,8 @@ def run_batched(args):
                                    f"detector U[128,1024]^2 x{args.scale}, seed 4",
                        "voxels": int(sum(np.prod(g.shape) for g in geoms)),
                        "rays": int(sum(g.nv * g.na * g.nb for g in geoms)), "tiles": bp.tiles},
-            "extras": {"intersections_per_iteration": 2 * inter,
+            "extras": {"strategy": bp.strategy, "strategy_step_ms": bp.timings,
+                       "intersections_per_iteration": 2 * inter,
                        "batched_intersections_per_s": 2 * inter / t_batch,
                        "sequential_device_s": t_seq, "plain_dropin_s": t_plain,
                        "speedup_vs_plain_dropin": t_plain / t_batch,

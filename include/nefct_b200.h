@@ -161,7 +161,8 @@ nefct_status nefct_cb_count_intersections(const nefct_cb_geom *g, uint32_t flags
                                           unsigned long long *count, void *stream);
 
 /* Batched cone-beam problems of uneven sizes: forward of every problem in
- * one persistent launch, transposes of every problem in another.  No
+ * one persistent launch, transposes of every problem in another (or one
+ * launch per problem, nefct_cb_batch_set_strategy).  No
  * counterpart in the reference (which projects one problem per op call,
  * e.g. project_t.py:153-160 even one view per call).  Work is tiled (32
  * detector columns x NEFCT_TUNE_CB_ROWS rows of one view), ordered longest
@@ -176,9 +177,9 @@ typedef struct nefct_cb_problem {
     float *back;               /* device [nz][ny][nx], transpose output (overwritten) */
 } nefct_cb_problem;
 typedef struct nefct_cb_batch nefct_cb_batch;
-/* Host-only: validates the problems, builds the tile order and returns the
- * device workspace size (descriptors, view tables, one volume copy per
- * problem). */
+/* Host-only: validates the problems (at most 96 per plan), builds the tile
+ * order and returns the device workspace size (view tables and one volume
+ * copy per problem; the problem descriptors travel as kernel parameters). */
 nefct_status nefct_cb_batch_plan(const nefct_cb_problem *problems, int32_t n, uint32_t flags,
                                  nefct_cb_batch **plan, size_t *workspace_bytes);
 /* Uploads the plan's tables into the caller's workspace (256-byte aligned)
@@ -186,9 +187,17 @@ nefct_status nefct_cb_batch_plan(const nefct_cb_problem *problems, int32_t n, ui
  * capturing them in a CUDA graph; the buffers named in the problems must stay
  * valid while the plan is used. */
 nefct_status nefct_cb_batch_bind(nefct_cb_batch *plan, void *workspace, size_t workspace_bytes, void *stream);
-nefct_status nefct_cb_batch_forward(const nefct_cb_batch *plan, void *stream);
-nefct_status nefct_cb_batch_backward(const nefct_cb_batch *plan, void *stream);
+nefct_status nefct_cb_batch_forward(nefct_cb_batch *plan, void *stream);
+nefct_status nefct_cb_batch_backward(nefct_cb_batch *plan, void *stream);
 int64_t nefct_cb_batch_tiles(const nefct_cb_batch *plan);   /* work tiles per launch */
+/* How forward/backward run the problems: one persistent launch over all
+ * tiles (NEFCT_BATCH_PERSISTENT), or the single-problem kernels once per
+ * problem (NEFCT_BATCH_PER_PROBLEM, the default: the persistent kernel holds
+ * its per-problem constants in registers and runs at lower occupancy, which
+ * only pays when problems are too small to fill the GPU). */
+#define NEFCT_BATCH_PERSISTENT  0
+#define NEFCT_BATCH_PER_PROBLEM 1
+nefct_status nefct_cb_batch_set_strategy(nefct_cb_batch *plan, int32_t strategy);
 void nefct_cb_batch_destroy(nefct_cb_batch *plan);
 
 /* LOR projector pair.  lors is [6][n] (rows x1 y1 z1 x2 y2 z2, each n

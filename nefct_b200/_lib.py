@@ -30,6 +30,7 @@ FDK_NO_WEIGHT = 0x100
 
 DET_FLAT, DET_CYL = 0, 1
 TUNE_CB_ROWS, TUNE_CB_ORDER = 0, 1
+BATCH_PERSISTENT, BATCH_PER_PROBLEM = 0, 1
 WIN_RAM_LAK, WIN_SHEPP_LOGAN, WIN_COSINE, WIN_HAMMING, WIN_HANN = 0, 1, 2, 3, 4
 WINDOWS = {"ram-lak": WIN_RAM_LAK, "shepp-logan": WIN_SHEPP_LOGAN, "cosine": WIN_COSINE,
            "hamming": WIN_HAMMING, "hann": WIN_HANN}
@@ -84,6 +85,7 @@ _PROTOS = {
     "nefct_cb_batch_forward": (_i32, [_vp, _vp]),
     "nefct_cb_batch_backward": (_i32, [_vp, _vp]),
     "nefct_cb_batch_tiles": (C.c_int64, [_vp]),
+    "nefct_cb_batch_set_strategy": (_i32, [_vp, _i32]),
     "nefct_cb_batch_destroy": (None, [_vp]),
     "nefct_lor_forward": (_i32, [C.POINTER(Grid), _vp, C.c_int64, _vp, _vp, _u32, _vp]),
     "nefct_lor_backward": (_i32, [C.POINTER(Grid), _vp, C.c_int64, _vp, _vp, _u32, _vp]),

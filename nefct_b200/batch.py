@@ -22,7 +22,7 @@ __all__ = ["BatchProjector"]
 
 class BatchProjector:
     def __init__(self, geoms: list[ops.ConeBeam], vols: list[torch.Tensor], sinos=None, grads=None, backs=None,
-                 flags: int = 0):
+                 flags: int = 0, strategy: str = "auto"):
         if len(geoms) != len(vols) or not geoms:
             raise ValueError("need one volume per geometry")
         dev = vols[0].device
@@ -55,6 +55,28 @@ class BatchProjector:
             _lib.check(lib.nefct_cb_batch_bind(plan, self.workspace.data_ptr(), nbytes.value,
                                                torch.cuda.current_stream(dev).cuda_stream))
         self.tiles = int(lib.nefct_cb_batch_tiles(plan))
+        self.timings = {}
+        if strategy == "auto":
+            strategy = self._pick()
+        self.set_strategy(strategy)
+
+    def set_strategy(self, strategy: str) -> None:
+        code = {"persistent": _lib.BATCH_PERSISTENT, "per-problem": _lib.BATCH_PER_PROBLEM}[strategy]
+        _lib.check(_lib.load().nefct_cb_batch_set_strategy(self._plan, code))
+        self.strategy = strategy
+
+    def _pick(self) -> str:
+        """Times one step with each strategy (after a warm-up) and returns the faster."""
+        for name in ("persistent", "per-problem"):
+            self.set_strategy(name)
+            self.step()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            self.step()
+            e1.record()
+            e1.synchronize()
+            self.timings[name] = e0.elapsed_time(e1)
+        return min(self.timings, key=self.timings.get)
 
     def _stream(self):
         return torch.cuda.current_stream(self.device).cuda_stream

@@ -1,4 +1,14 @@
-// Batched cone-beam problems of uneven sizes in one persistent launch.
+// Batched cone-beam problems of uneven sizes.
+//
+// Two strategies, picked per plan (nefct_cb_batch_set_strategy; the python
+// BatchProjector times both):
+//  * persistent -- every problem's tiles in one persistent launch per
+//    direction (described below);
+//  * per-problem -- the single-problem kernels launched once per problem.
+// The persistent kernel indexes its problem descriptor dynamically, so the
+// per-problem constants that the single-problem kernels read as
+// constant-bank operands occupy registers (~100 vs ~56), halving occupancy;
+// it pays off when problems are too small to fill the GPU one at a time.
 //
 // A plan holds, for n problems (each with its own grid, views, detector and
 // scanner), a table of work tiles -- 32 detector columns x R rows of one
@@ -12,7 +22,8 @@
 // stream-ordered and capturable in a CUDA graph after nefct_cb_batch_bind.
 //
 // Device workspace (caller-owned), 256-byte aligned sections:
-//   counters[2] | descriptors[n] | tile offsets[n+1] | view tables | per-problem y-fastest volume
+//   counters[4] | view tables | per-problem y-fastest volume
+// (problem descriptors and tile offsets travel as kernel parameters)
 // The y-fastest copy holds the transposed volume during the forward and
 // the accumulator of x-driven rays during the transpose.
 #include <algorithm>
@@ -25,6 +36,10 @@
 namespace nefct {
 
 nefct_status check_cb_geom(const nefct_cb_geom *g);
+nefct_status cb_forward_launches(const nefct_cb_geom *g, const float *vol, const float *volT, float *sino,
+                                 uint32_t flags, cudaStream_t s);
+nefct_status cb_backward_launches(const nefct_cb_geom *g, const float *sino, float *out, float *outT,
+                                  uint32_t flags, cudaStream_t s);
 
 struct BatchDesc {
     GridDev<float> g;
@@ -39,8 +54,22 @@ struct BatchDesc {
     float *volT;                         // y-fastest copy / accumulator
 };
 
+// Descriptors and tile offsets travel in the kernel parameter space (read
+// through the constant cache, like the single-problem kernels' parameters),
+// which bounds the problems per plan.
+static constexpr int kMaxBatch = 96;
+struct BatchArgs {
+    BatchDesc d[kMaxBatch];
+    long long t0[kMaxBatch + 1];
+    int n;
+    long long begin, end;
+    unsigned long long *counter;
+};
+
 struct BatchPlan {
-    std::vector<nefct_cb_problem> probs;   // caller order
+    std::vector<nefct_cb_problem> probs;   // caller order; geom.angles/z_offsets point into the copies below
+    std::vector<std::vector<float>> angles, offsets;
+    int strategy = NEFCT_BATCH_PER_PROBLEM;
     std::vector<int> order;                // plan order -> caller index
     std::vector<BatchDesc> desc;           // plan order (device pointers filled at bind)
     std::vector<long long> t0;             // tile offsets, n + 1
@@ -48,15 +77,18 @@ struct BatchPlan {
     std::vector<size_t> view_off, vol_off; // float offsets in the workspace sections
     uint32_t flags = 0;
     int rows = 4;
+    long long split = 0;                   // tiles of cubic-voxel problems come first
     size_t off_desc = 0, off_t0 = 0, off_views = 0, off_vols = 0, bytes = 0;
     unsigned char *ws = nullptr;           // bound workspace
     int grid_blocks = 0;
+    BatchArgs *args = nullptr;             // launch parameters (host copy)
+    ~BatchPlan() { delete args; }
 };
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// Tile `item` of the plan -> (problem, view, first column, first row).
-__device__ __forceinline__ int find_problem(const long long *__restrict__ t0, int n, long long item)
+// Tile `item` of the plan -> its problem (largest p with t0[p] <= item).
+__device__ __forceinline__ int find_problem(const long long *t0, int n, long long item)
 {
     int lo = 0, hi = n - 1;
     while (lo < hi) {
@@ -67,21 +99,21 @@ __device__ __forceinline__ int find_problem(const long long *__restrict__ t0, in
     return lo;
 }
 
-template <bool FWD>
-__global__ void __launch_bounds__(256) batch_kernel(const BatchDesc *__restrict__ d, const long long *__restrict__ t0,
-                                                    int n, unsigned long long *counter)
+// One persistent launch serves tiles [begin, end) of problems that share
+// the DIV variant (cubic voxels or not).
+template <bool FWD, bool DIV>
+__global__ void __launch_bounds__(256) batch_kernel(const __grid_constant__ BatchArgs a)
 {
     __shared__ long long s_item;
-    const long long total = t0[n];
     for (;;) {
-        if (threadIdx.x == 0 && threadIdx.y == 0) s_item = (long long)atomicAdd(counter, 1ull);
+        if (threadIdx.x == 0 && threadIdx.y == 0) s_item = a.begin + (long long)atomicAdd(a.counter, 1ull);
         __syncthreads();
         const long long item = s_item;
         __syncthreads();                  // all threads read s_item before the next ticket
-        if (item >= total) return;        // uniform across the CTA
-        const int p = find_problem(t0, n, item);
-        const BatchDesc &P = d[p];
-        const long long local = item - t0[p];
+        if (item >= a.end) return;        // uniform across the CTA
+        const int p = find_problem(a.t0, a.n, item);
+        const BatchDesc &P = a.d[p];
+        const long long local = item - a.t0[p];
         const int ct = (int)(local % P.tiles_a);
         const long long rest = local / P.tiles_a;
         const int band = (int)(rest % P.tiles_b);
@@ -92,24 +124,51 @@ __global__ void __launch_bounds__(256) batch_kernel(const BatchDesc *__restrict_
         cb_ray(P.rg, P.cs[iv], P.sn[iv], P.off[iv], ia, ib, r);
         const size_t id = ((size_t)iv * P.nb + ib) * P.na + ia;
         if (FWD) {
-            const float acc = P.cubic ? ray_forward<float, false>(P.g, r, P.flags, P.vol, P.volT)
-                                      : ray_forward<float, true>(P.g, r, P.flags, P.vol, P.volT);
-            P.sino[id] = acc;
+            P.sino[id] = ray_forward<float, DIV>(P.g, r, P.flags, P.vol, P.volT);
         } else {
             const float y = P.grad[id];
             if (y == 0.f) continue;
-            if (P.cubic) ray_backward<float, false>(P.g, r, P.flags, y, P.back, P.volT);
-            else ray_backward<float, true>(P.g, r, P.flags, y, P.back, P.volT);
+            ray_backward<float, DIV>(P.g, r, P.flags, y, P.back, P.volT);
         }
     }
 }
 
-static nefct_status batch_launch(const BatchPlan *b, bool fwd, cudaStream_t s)
+// Per-problem strategy: the single-problem kernels launched once per problem
+// (their scanner constants as kernel parameters), stream-ordered.
+static nefct_status batch_per_problem(BatchPlan *b, bool fwd, cudaStream_t s)
+{
+    const int n = (int)b->desc.size();
+    for (int k = 0; k < n; ++k) {
+        const BatchDesc &D = b->desc[k];
+        const nefct_cb_geom &g = b->probs[b->order[k]].geom;
+        const size_t nvox = (size_t)D.g.nx * D.g.ny * D.g.nz;
+        dim3 tg((D.g.nx + 31) / 32, (D.g.ny + 31) / 32, D.g.nz);
+        nefct_status st;
+        if (fwd) {
+            transpose_xy_kernel<float><<<tg, dim3(32, 8), 0, s>>>(D.vol, D.volT, D.g.nx, D.g.ny);
+            NEFCT_CHECK_LAUNCH("transpose_xy_kernel (batch)");
+            st = cb_forward_launches(&g, D.vol, D.volT, D.sino, D.flags, s);
+        } else {
+            NEFCT_CHECK_CUDA(cudaMemsetAsync(D.back, 0, nvox * sizeof(float), s));
+            NEFCT_CHECK_CUDA(cudaMemsetAsync(D.volT, 0, nvox * sizeof(float), s));
+            st = cb_backward_launches(&g, D.grad, D.back, D.volT, D.flags, s);
+            if (!st) {
+                fold_add_kernel<float><<<tg, dim3(32, 8), 0, s>>>(D.volT, D.back, D.g.nx, D.g.ny);
+                NEFCT_CHECK_LAUNCH("fold_add_kernel (batch)");
+            }
+        }
+        if (st) return st;
+    }
+    return NEFCT_OK;
+}
+
+static nefct_status batch_launch(BatchPlan *b, bool fwd, cudaStream_t s)
 {
     if (!b || !b->ws) return fail(NEFCT_ERR_INVALID, "batch plan is not bound to a workspace");
+    if (b->strategy == NEFCT_BATCH_PER_PROBLEM) return batch_per_problem(b, fwd, s);
     const int n = (int)b->desc.size();
-    unsigned long long *counter = (unsigned long long *)b->ws + (fwd ? 0 : 1);
-    NEFCT_CHECK_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
+    unsigned long long *counter = (unsigned long long *)b->ws + (fwd ? 0 : 2);
+    NEFCT_CHECK_CUDA(cudaMemsetAsync(counter, 0, 2 * sizeof(unsigned long long), s));
     for (int i = 0; i < n; ++i) {
         const BatchDesc &D = b->desc[i];
         const size_t nvox = (size_t)D.g.nx * D.g.ny * D.g.nz;
@@ -122,11 +181,21 @@ static nefct_status batch_launch(const BatchPlan *b, bool fwd, cudaStream_t s)
             NEFCT_CHECK_CUDA(cudaMemsetAsync(D.volT, 0, nvox * sizeof(float), s));
         }
     }
-    const BatchDesc *dd = (const BatchDesc *)(b->ws + b->off_desc);
-    const long long *t0 = (const long long *)(b->ws + b->off_t0);
-    if (fwd) batch_kernel<true><<<b->grid_blocks, dim3(32, b->rows), 0, s>>>(dd, t0, n, counter);
-    else batch_kernel<false><<<b->grid_blocks, dim3(32, b->rows), 0, s>>>(dd, t0, n, counter);
-    NEFCT_CHECK_LAUNCH("batch_kernel");
+    const long long total = b->t0.back();
+    const dim3 blk(32, b->rows);
+    BatchArgs &a = *b->args;
+    if (b->split > 0) {
+        a.begin = 0; a.end = b->split; a.counter = counter;
+        if (fwd) batch_kernel<true, false><<<b->grid_blocks, blk, 0, s>>>(a);
+        else batch_kernel<false, false><<<b->grid_blocks, blk, 0, s>>>(a);
+        NEFCT_CHECK_LAUNCH("batch_kernel (cubic voxels)");
+    }
+    if (b->split < total) {
+        a.begin = b->split; a.end = total; a.counter = counter + 1;
+        if (fwd) batch_kernel<true, true><<<b->grid_blocks, blk, 0, s>>>(a);
+        else batch_kernel<false, true><<<b->grid_blocks, blk, 0, s>>>(a);
+        NEFCT_CHECK_LAUNCH("batch_kernel (other voxels)");
+    }
     if (!fwd) {
         for (int i = 0; i < n; ++i) {
             const BatchDesc &D = b->desc[i];
@@ -152,6 +221,7 @@ nefct_status nefct_cb_batch_plan(const nefct_cb_problem *problems, int32_t n, ui
     if (!plan || !workspace_bytes) return fail(NEFCT_ERR_INVALID, "plan and workspace_bytes must be non-NULL");
     *plan = nullptr;
     if (n < 1 || !problems) return fail(NEFCT_ERR_INVALID, "need at least one problem");
+    if (n > kMaxBatch) return fail(NEFCT_ERR_INVALID, "at most %d problems per batch plan (got %d)", kMaxBatch, n);
     if (flags & ~(NEFCT_TIE_GT | NEFCT_SKIP_SHORT | NEFCT_NO_INV_L2))
         return fail(NEFCT_ERR_INVALID, "flags 0x%x not supported by the batch", flags);
     for (int i = 0; i < n; ++i) {
@@ -165,12 +235,30 @@ nefct_status nefct_cb_batch_plan(const nefct_cb_problem *problems, int32_t n, ui
     }
     nefct_cb_batch *b = new nefct_cb_batch();
     b->probs.assign(problems, problems + n);
+    b->angles.resize(n);
+    b->offsets.resize(n);
+    for (int i = 0; i < n; ++i) {
+        nefct_cb_geom &g = b->probs[i].geom;
+        b->angles[i].assign(g.angles, g.angles + g.nv);
+        g.angles = b->angles[i].data();
+        if (g.z_offsets) {
+            b->offsets[i].assign(g.z_offsets, g.z_offsets + g.nv);
+            g.z_offsets = b->offsets[i].data();
+        }
+    }
     b->flags = flags;
     b->rows = tune_get(NEFCT_TUNE_CB_ROWS);
-    // longest rays first: a tile's cost grows with the slab count of its rays
+    // cubic-voxel problems first (one kernel variant each), longest rays
+    // first within each group: a tile's cost grows with its rays' slab count
+    auto cubic = [&](int i) {
+        const GridDev<float> g = make_grid_dev<float>(problems[i].geom.grid);
+        return g.dy == 1.f && g.dz == 1.f;
+    };
     b->order.resize(n);
     std::iota(b->order.begin(), b->order.end(), 0);
     std::stable_sort(b->order.begin(), b->order.end(), [&](int a, int c) {
+        const bool ca = cubic(a), cc = cubic(c);
+        if (ca != cc) return ca;
         const nefct_grid &ga = problems[a].geom.grid, &gc = problems[c].geom.grid;
         return std::max(ga.nx, ga.ny) > std::max(gc.nx, gc.ny);
     });
@@ -190,6 +278,7 @@ nefct_status nefct_cb_batch_plan(const nefct_cb_problem *problems, int32_t n, ui
         D.cubic = D.g.dy == 1.f && D.g.dz == 1.f;
         D.flags = flags;
         b->t0[k + 1] = b->t0[k] + (long long)D.tiles_a * D.tiles_b * g.nv;
+        if (D.cubic) b->split = b->t0[k + 1];
         b->view_off[k] = views;
         views += 3 * (size_t)g.nv;
         b->vol_off[k] = vols;
@@ -205,9 +294,9 @@ nefct_status nefct_cb_batch_plan(const nefct_cb_problem *problems, int32_t n, ui
             v[2 * g.nv + i] = g.z_offsets ? g.z_offsets[i] : 0.f;
         }
     }
-    b->off_desc = align256(2 * sizeof(unsigned long long));
-    b->off_t0 = b->off_desc + align256(n * sizeof(BatchDesc));
-    b->off_views = b->off_t0 + align256((n + 1) * sizeof(long long));
+    b->off_desc = align256(4 * sizeof(unsigned long long));
+    b->off_t0 = b->off_desc;
+    b->off_views = b->off_desc;
     b->off_vols = b->off_views + align256(views * sizeof(float));
     b->bytes = b->off_vols + vols * sizeof(float);
     *workspace_bytes = b->bytes;
@@ -232,8 +321,10 @@ nefct_status nefct_cb_batch_bind(nefct_cb_batch *b, void *workspace, size_t byte
         D.volT = (float *)(ws + b->off_vols) + b->vol_off[k];
     }
     cudaStream_t s = (cudaStream_t)stream;
-    NEFCT_CHECK_CUDA(cudaMemcpyAsync(ws + b->off_desc, b->desc.data(), n * sizeof(BatchDesc), cudaMemcpyHostToDevice, s));
-    NEFCT_CHECK_CUDA(cudaMemcpyAsync(ws + b->off_t0, b->t0.data(), (n + 1) * sizeof(long long), cudaMemcpyHostToDevice, s));
+    if (!b->args) b->args = new BatchArgs();
+    std::copy(b->desc.begin(), b->desc.end(), b->args->d);
+    std::copy(b->t0.begin(), b->t0.end(), b->args->t0);
+    b->args->n = n;
     NEFCT_CHECK_CUDA(cudaMemcpyAsync(ws + b->off_views, b->views.data(), b->views.size() * sizeof(float),
                                      cudaMemcpyHostToDevice, s));
     // the copies read the plan's host memory: finish them before returning
@@ -241,25 +332,37 @@ nefct_status nefct_cb_batch_bind(nefct_cb_batch *b, void *workspace, size_t byte
     int dev = 0, sms = 0, per_sm = 0;
     NEFCT_CHECK_CUDA(cudaGetDevice(&dev));
     NEFCT_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    NEFCT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<true>, 32 * b->rows, 0));
-    int per_sm_b = 0;
-    NEFCT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_b, batch_kernel<false>, 32 * b->rows, 0));
-    b->grid_blocks = sms * std::max(1, std::min(per_sm, per_sm_b));
+    int lo = 1 << 30;
+    for (const void *k : {(const void *)batch_kernel<true, false>, (const void *)batch_kernel<true, true>,
+                          (const void *)batch_kernel<false, false>, (const void *)batch_kernel<false, true>}) {
+        NEFCT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * b->rows, 0));
+        lo = std::min(lo, per_sm);
+    }
+    b->grid_blocks = sms * std::max(1, lo);
     b->ws = ws;
     return NEFCT_OK;
 }
 
-nefct_status nefct_cb_batch_forward(const nefct_cb_batch *b, void *stream)
+nefct_status nefct_cb_batch_forward(nefct_cb_batch *b, void *stream)
 {
     return batch_launch(b, true, (cudaStream_t)stream);
 }
 
-nefct_status nefct_cb_batch_backward(const nefct_cb_batch *b, void *stream)
+nefct_status nefct_cb_batch_backward(nefct_cb_batch *b, void *stream)
 {
     return batch_launch(b, false, (cudaStream_t)stream);
 }
 
 int64_t nefct_cb_batch_tiles(const nefct_cb_batch *b) { return b ? (int64_t)b->t0.back() : -1; }
+
+nefct_status nefct_cb_batch_set_strategy(nefct_cb_batch *b, int32_t strategy)
+{
+    if (!b) return fail(NEFCT_ERR_INVALID, "plan is NULL");
+    if (strategy != NEFCT_BATCH_PERSISTENT && strategy != NEFCT_BATCH_PER_PROBLEM)
+        return fail(NEFCT_ERR_INVALID, "unknown batch strategy %d", strategy);
+    b->strategy = strategy;
+    return NEFCT_OK;
+}
 
 void nefct_cb_batch_destroy(nefct_cb_batch *b) { delete b; }
 

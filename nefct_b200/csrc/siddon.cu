@@ -233,6 +233,49 @@ static nefct_status transpose_xy(const T *in, T *out, const nefct_grid &g, cudaS
     return NEFCT_OK;
 }
 
+// Launches of the forward / transpose kernels for one problem whose
+// y-fastest volume copy (forward) or accumulator (transpose) is given; no
+// transpose, memset or fold.  Used by the batch's per-problem strategy.
+nefct_status cb_forward_launches(const nefct_cb_geom *g, const float *vol, const float *volT, float *sino,
+                                 uint32_t flags, cudaStream_t s)
+{
+    CBParams<float> p;
+    fill_cb_params(p, g, flags);
+    p.vol = vol;
+    p.volT = volT;
+    p.out = sino;
+    for (int v0 = 0; v0 < g->nv; v0 += ViewTable<float>::kMax) {
+        const int nvc = std::min(ViewTable<float>::kMax, g->nv - v0);
+        fill_views(p, g, v0, nvc);
+        dim3 grid, block;
+        cb_shape(p, g->na, g->nb, nvc, grid, block);
+        if (cubic(p.g)) cb_forward_kernel<float, false><<<grid, block, 0, s>>>(p);
+        else cb_forward_kernel<float, true><<<grid, block, 0, s>>>(p);
+        NEFCT_CHECK_LAUNCH("cb_forward_kernel");
+    }
+    return NEFCT_OK;
+}
+
+nefct_status cb_backward_launches(const nefct_cb_geom *g, const float *sino, float *out, float *outT,
+                                  uint32_t flags, cudaStream_t s)
+{
+    CBParams<float> p;
+    fill_cb_params(p, g, flags);
+    p.sino = sino;
+    p.out = out;
+    p.outT = outT;
+    for (int v0 = 0; v0 < g->nv; v0 += ViewTable<float>::kMax) {
+        const int nvc = std::min(ViewTable<float>::kMax, g->nv - v0);
+        fill_views(p, g, v0, nvc);
+        dim3 grid, block;
+        cb_shape(p, g->na, g->nb, nvc, grid, block);
+        if (cubic(p.g)) cb_backward_kernel<float, false><<<grid, block, 0, s>>>(p);
+        else cb_backward_kernel<float, true><<<grid, block, 0, s>>>(p);
+        NEFCT_CHECK_LAUNCH("cb_backward_kernel");
+    }
+    return NEFCT_OK;
+}
+
 template <typename T>
 static nefct_status cb_forward_impl(const nefct_cb_geom *g, const T *vol, T *sino, uint32_t flags, void *ws,
                                     size_t wsb, cudaStream_t s)

@@ -31,10 +31,11 @@ def _problems(dev):
     return geoms, vols, grads
 
 
+@pytest.mark.parametrize("strategy", ["persistent", "per-problem"])
 @pytest.mark.parametrize("flags", [0, nb._lib.LINE_INTEGRAL])
-def test_batch_matches_per_problem(cuda, flags):
+def test_batch_matches_per_problem(cuda, flags, strategy):
     geoms, vols, grads = _problems(cuda)
-    bp = BatchProjector(geoms, vols, grads=grads, flags=flags)
+    bp = BatchProjector(geoms, vols, grads=grads, flags=flags, strategy=strategy)
     bp.step()
     torch.cuda.synchronize()
     for g, v, gr, s, b in zip(geoms, vols, grads, bp.sinos, bp.backs):
@@ -43,9 +44,10 @@ def test_batch_matches_per_problem(cuda, flags):
         assert_parity(b.cpu().numpy(), ops.cb_backward(gr, g, flags).cpu().numpy())
 
 
-def test_batch_graph_replay(cuda):
+@pytest.mark.parametrize("strategy", ["persistent", "per-problem"])
+def test_batch_graph_replay(cuda, strategy):
     geoms, vols, grads = _problems(cuda)
-    bp = BatchProjector(geoms, vols, grads=grads)
+    bp = BatchProjector(geoms, vols, grads=grads, strategy=strategy)
     graph = bp.capture()
     for b in bp.backs:
         b.zero_()
@@ -58,3 +60,9 @@ def test_batch_graph_replay(cuda):
         assert torch.equal(s, ops.cb_forward(v, g))
         assert_parity(b.cpu().numpy(), ops.cb_backward(gr, g).cpu().numpy())
     assert bp.tiles > 0
+
+
+def test_batch_auto_strategy_times_both(cuda):
+    geoms, vols, grads = _problems(cuda)
+    bp = BatchProjector(geoms, vols, grads=grads)
+    assert set(bp.timings) == {"persistent", "per-problem"} and bp.strategy in bp.timings

@@ -101,6 +101,8 @@ typedef struct nefct_cb_geom {
 #define NEFCT_Q5            0x08u /* extra 1/L on y-driven three-voxel middle weights (cpp/siddon :292,:313) */
 #define NEFCT_Q8_INDEX      0x10u /* cylindrical backprojection reads the sinogram at ia + iv*na + ib*na*nb (:830) */
 #define NEFCT_NO_TRANSPOSE  0x20u /* x-driven rays read the x-fastest volume directly: no workspace, slower */
+#define NEFCT_DETERMINISTIC 0x40u /* backward: bitwise reproducible sums (64-bit fixed point, see nefct_cb_backward);
+                                     the forward is deterministic anyway and ignores it */
 
 /* presets */
 #define NEFCT_REF_FORWARD        0u                                              /* siddon_3d project_device */
@@ -111,7 +113,9 @@ typedef struct nefct_cb_geom {
 
 /* Bytes of workspace nefct_cb_forward / nefct_cb_backward need for this
  * geometry and flags (a y-fastest copy of the volume; 0 with
- * NEFCT_NO_TRANSPOSE).  Host-only, no CUDA call. */
+ * NEFCT_NO_TRANSPOSE; with NEFCT_DETERMINISTIC the backward's two 64-bit
+ * accumulators).  FP64 calls need twice the non-deterministic size.
+ * Host-only, no CUDA call. */
 size_t nefct_cb_workspace_bytes(const nefct_cb_geom *g, uint32_t flags);
 
 /* Cone-beam forward projection vol -> sino.  Replaces ProjectFlat /
@@ -125,7 +129,13 @@ nefct_status nefct_cb_forward(const nefct_cb_geom *g, const float *vol, float *s
 /* Cone-beam backprojection sino -> vol (vol is overwritten).  With the same
  * flags as a forward call it is that forward's exact transpose; with
  * NEFCT_REF_BACKPROJECT it reproduces BackProjectFlat / BackProjectCyli
- * (siddon.cc:44-80, 226-348; siddon.cu.cc:450-890). */
+ * (siddon.cc:44-80, 226-348; siddon.cu.cc:450-890).
+ * Sums are float atomics (order not fixed) unless NEFCT_DETERMINISTIC: then
+ * every contribution is scaled by a power of two chosen from max|sino| and a
+ * bound on the weights (so no sum can exceed 2^61), rounded to a 64-bit
+ * integer and reduced with integer atomics, and the sums are converted once
+ * -- bitwise identical across runs, with rounding far below float sums.
+ * Float32 only; NaN/Inf in sino are not supported in that mode. */
 nefct_status nefct_cb_backward(const nefct_cb_geom *g, const float *sino, float *vol, uint32_t flags,
                                void *workspace, size_t workspace_bytes, void *stream);
 

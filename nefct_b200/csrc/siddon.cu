@@ -32,6 +32,8 @@ template <typename T> struct CBParams {
     const T *sino;       // backward source, full sinogram
     T *out;              // forward: full sinogram; backward: x-fastest volume
     T *outT;             // backward: y-fastest accumulator, or nullptr
+    unsigned long long *fix, *fixT;   // deterministic backward: integer accumulators
+    const float *fix_scale;           // deterministic backward: power-of-two scale (device)
     unsigned long long *count;
     ViewTable<T> tab;
 };
@@ -99,6 +101,79 @@ __global__ void __launch_bounds__(256) cb_count_kernel(const __grid_constant__ C
     if ((threadIdx.x & 31) == 0 && n) atomicAdd(p.count, (unsigned long long)n);
 }
 
+// ---------------- deterministic transpose (fixed point) ----------------
+
+template <bool DIV>
+__global__ void __launch_bounds__(256) cb_backward_fixed_kernel(const __grid_constant__ CBParams<float> p)
+{
+    int ia, ib, iv;
+    cb_cell(p, ia, ib, iv);
+    if (ia >= p.na || ib >= p.nb) return;
+    const size_t total = (size_t)p.na * p.nb * p.nv_total;
+    const size_t vg = (size_t)(p.v0 + iv);
+    const size_t id = (p.flags & NEFCT_Q8_INDEX) ? (size_t)ia + vg * p.na + (size_t)ib * p.na * p.nb
+                                                 : vg * p.na * p.nb + (size_t)ib * p.na + ia;
+    const float y = id < total ? p.sino[id] : 0.f;
+    if (y == 0.f) return;
+    float r[6];
+    cb_ray(p, ia, ib, iv, r);
+    Walk<float> w;
+    if (!setup_walk(p.g, r, p.flags, w)) return;
+    const float scale = *p.fix_scale;
+    const int sw = p.g.nx * p.g.ny;
+    if (!w.xdrive) scatter_walk_fixed<float, DIV, true>(w, p.g, p.fix, p.g.nx, 1, sw, y, scale);
+    else if (p.fixT) scatter_walk_fixed<float, DIV, true>(w, p.g, p.fixT, p.g.ny, 1, sw, y, scale);
+    else scatter_walk_fixed<float, DIV, false>(w, p.g, p.fix, 1, p.g.nx, sw, y, scale);
+}
+
+// max |x| as float bits (non-negative floats order like their bit patterns)
+__global__ void __launch_bounds__(256) maxabs_kernel(const float *__restrict__ x, size_t n, unsigned *out)
+{
+    unsigned m = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        m = max(m, __float_as_uint(fabsf(x[i])));
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+// scale = 2^k with k the largest integer such that bound * max|y| * 2^k <= 2^61,
+// where bound >= (rays) * (largest weight); then no per-voxel sum of
+// |contribution| * scale can exceed 2^61.
+__global__ void fixed_scale_kernel(const unsigned *maxbits, double bound, float *scale)
+{
+    const double B = bound * (double)__uint_as_float(*maxbits);
+    int k = 0;
+    if (B > 0.0 && B < 1e300) k = (int)floor(61.0 - log2(B));
+    k = max(-126, min(127, k));
+    *scale = ldexpf(1.0f, k);
+}
+
+// vol[z][y][x] = (accN[z][y][x] + accT[z][x][y]) / scale, integer sum first
+__global__ void __launch_bounds__(256) fixed_fold_kernel(const unsigned long long *__restrict__ accN,
+                                                         const unsigned long long *__restrict__ accT, int nx, int ny,
+                                                         const float *scale, float *__restrict__ vol)
+{
+    __shared__ unsigned long long tile[32][33];
+    const size_t plane = (size_t)nx * ny * blockIdx.z;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    if (accT) {
+        for (int j = threadIdx.y; j < 32; j += 8) {
+            const int y = y0 + threadIdx.x, x = x0 + j;
+            if (x < nx && y < ny) tile[j][threadIdx.x] = accT[plane + (size_t)x * ny + y];
+        }
+    }
+    __syncthreads();
+    const double inv = 1.0 / (double)*scale;
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int x = x0 + threadIdx.x, y = y0 + j;
+        if (x < nx && y < ny) {
+            unsigned long long v = accN[plane + (size_t)y * nx + x];
+            if (accT) v += tile[threadIdx.x][j];
+            vol[plane + (size_t)y * nx + x] = (float)((double)(long long)v * inv);
+        }
+    }
+}
+
 // ---------------- LOR projector pair (cpp/siddon) ----------------
 
 template <typename T> struct LorParams {
@@ -162,7 +237,7 @@ template <typename T> static void cb_shape(CBParams<T> &p, int na, int nb, int n
 template <typename T> static bool cubic(const GridDev<T> &g) { return g.dy == (T)1 && g.dz == (T)1; }
 
 static const uint32_t kWalkFlags = NEFCT_TIE_GT | NEFCT_SKIP_SHORT | NEFCT_NO_INV_L2 | NEFCT_Q5 |
-                                   NEFCT_Q8_INDEX | NEFCT_NO_TRANSPOSE;
+                                   NEFCT_Q8_INDEX | NEFCT_NO_TRANSPOSE | NEFCT_DETERMINISTIC;
 
 static nefct_status check_grid(const nefct_grid &g)
 {
@@ -313,6 +388,71 @@ static nefct_status cb_forward_impl(const nefct_cb_geom *g, const T *vol, T *sin
     return NEFCT_OK;
 }
 
+// Upper bound of (rays) x (largest contribution weight) for the fixed-point
+// scale: |kv| <= 1 by the choice of driving axis; the transverse
+// source-detector distance is >= src_det (flat: sqrt(src_det^2 + a^2);
+// cylindrical: exactly src_det), so |kw| <= sqrt(2) max|b| / src_det and
+// L >= src_det / dx in voxel units.
+static double fixed_bound(const nefct_cb_geom *g, uint32_t flags)
+{
+    const double dx = (double)g->grid.sx / g->grid.nx;
+    const double half = g->nb * (double)g->db / 2.0;
+    const double b0 = fabs((0.0 + g->b_shift) * g->db - half);
+    const double b1 = fabs((g->nb - 1.0 + g->b_shift) * g->db - half);
+    const double kw = sqrt(2.0) * std::max(b0, b1) / g->src_det;
+    double W = sqrt(2.0 + kw * kw) * dx;
+    if (!(flags & NEFCT_NO_INV_L2)) W *= (dx / g->src_det) * (dx / g->src_det);
+    return (double)g->na * g->nb * g->nv * W * 1.001;
+}
+
+size_t cb_fixed_workspace(const nefct_cb_geom *g, uint32_t flags)
+{
+    const size_t nvox = (size_t)g->grid.nx * g->grid.ny * g->grid.nz;
+    return 256 + nvox * sizeof(unsigned long long) * ((flags & NEFCT_NO_TRANSPOSE) ? 1 : 2);
+}
+
+static nefct_status cb_backward_fixed_impl(const nefct_cb_geom *g, const float *sino, float *vol, uint32_t flags,
+                                           void *ws, size_t wsb, cudaStream_t s)
+{
+    if (flags & NEFCT_Q5) return fail(NEFCT_ERR_UNSUPPORTED, "NEFCT_Q5 is not available with NEFCT_DETERMINISTIC");
+    if (!(g->src_det > 0.f)) return fail(NEFCT_ERR_INVALID, "deterministic transpose needs src_det > 0");
+    const size_t nvox = (size_t)g->grid.nx * g->grid.ny * g->grid.nz;
+    const bool tr = !(flags & NEFCT_NO_TRANSPOSE);
+    const size_t need = cb_fixed_workspace(g, flags);
+    if (!ws || wsb < need)
+        return fail(NEFCT_ERR_WORKSPACE, "deterministic backward needs %zu workspace bytes, got %zu", need, wsb);
+    unsigned char *w = (unsigned char *)ws;
+    unsigned *maxbits = (unsigned *)w;
+    float *scale = (float *)(w + 16);
+    unsigned long long *accN = (unsigned long long *)(w + 256);
+    unsigned long long *accT = tr ? accN + nvox : nullptr;
+    NEFCT_CHECK_CUDA(cudaMemsetAsync(w, 0, need, s));
+    const size_t ns = (size_t)g->na * g->nb * g->nv;
+    maxabs_kernel<<<(unsigned)std::min<size_t>((ns + 255) / 256, 148 * 16), 256, 0, s>>>(sino, ns, maxbits);
+    NEFCT_CHECK_LAUNCH("maxabs_kernel");
+    fixed_scale_kernel<<<1, 1, 0, s>>>(maxbits, fixed_bound(g, flags), scale);
+    NEFCT_CHECK_LAUNCH("fixed_scale_kernel");
+    CBParams<float> p;
+    fill_cb_params(p, g, flags);
+    p.sino = sino;
+    p.fix = accN;
+    p.fixT = accT;
+    p.fix_scale = scale;
+    for (int v0 = 0; v0 < g->nv; v0 += ViewTable<float>::kMax) {
+        const int nvc = std::min(ViewTable<float>::kMax, g->nv - v0);
+        fill_views(p, g, v0, nvc);
+        dim3 grid, block;
+        cb_shape(p, g->na, g->nb, nvc, grid, block);
+        if (cubic(p.g)) cb_backward_fixed_kernel<false><<<grid, block, 0, s>>>(p);
+        else cb_backward_fixed_kernel<true><<<grid, block, 0, s>>>(p);
+        NEFCT_CHECK_LAUNCH("cb_backward_fixed_kernel");
+    }
+    dim3 grid((g->grid.nx + 31) / 32, (g->grid.ny + 31) / 32, g->grid.nz);
+    fixed_fold_kernel<<<grid, dim3(32, 8), 0, s>>>(accN, accT, g->grid.nx, g->grid.ny, scale, vol);
+    NEFCT_CHECK_LAUNCH("fixed_fold_kernel");
+    return NEFCT_OK;
+}
+
 template <typename T>
 static nefct_status cb_backward_impl(const nefct_cb_geom *g, const T *sino, T *vol, uint32_t flags, void *ws,
                                      size_t wsb, cudaStream_t s)
@@ -321,6 +461,11 @@ static nefct_status cb_backward_impl(const nefct_cb_geom *g, const T *sino, T *v
     if (st) return st;
     if (!vol || !sino) return fail(NEFCT_ERR_INVALID, "vol and sino must be non-NULL");
     if (flags & ~kWalkFlags) return fail(NEFCT_ERR_INVALID, "unknown flag bits 0x%x", flags & ~kWalkFlags);
+    if (flags & NEFCT_DETERMINISTIC) {
+        if (sizeof(T) != sizeof(float))
+            return fail(NEFCT_ERR_UNSUPPORTED, "NEFCT_DETERMINISTIC is available for float32 only");
+        return cb_backward_fixed_impl(g, (const float *)sino, (float *)vol, flags, ws, wsb, s);
+    }
     const size_t nvox = (size_t)g->grid.nx * g->grid.ny * g->grid.nz;
     const bool tr = !(flags & NEFCT_NO_TRANSPOSE);
     if (tr && (!ws || wsb < nvox * sizeof(T)))
@@ -476,7 +621,9 @@ extern "C" {
 
 size_t nefct_cb_workspace_bytes(const nefct_cb_geom *g, uint32_t flags)
 {
-    if (!g || (flags & NEFCT_NO_TRANSPOSE)) return 0;
+    if (!g || g->grid.nx < 1 || g->grid.ny < 1 || g->grid.nz < 1) return 0;
+    if (flags & NEFCT_DETERMINISTIC) return cb_fixed_workspace(g, flags);
+    if (flags & NEFCT_NO_TRANSPOSE) return 0;
     return (size_t)(g->grid.nx > 0 ? g->grid.nx : 0) * (size_t)(g->grid.ny > 0 ? g->grid.ny : 0) *
            (size_t)(g->grid.nz > 0 ? g->grid.nz : 0) * sizeof(float);
 }

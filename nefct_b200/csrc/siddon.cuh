@@ -371,6 +371,35 @@ __device__ __forceinline__ void scatter_walk(const Walk<T> &w, const GridDev<T> 
     else scatter_walk_t<T, DIV, false, SV1, Q5>(w, g, base, su, sv, sw, value);
 }
 
+// Deterministic transpose: each contribution value * weight is scaled by
+// a power of two (exact) and rounded to a 64-bit integer; integer sums do
+// not depend on the order of the reductions, so the result is bitwise
+// reproducible.  The caller picks the scale so that no sum can overflow.
+__device__ __forceinline__ long long to_fixed(float v) { return __float2ll_rn(v); }
+__device__ __forceinline__ long long to_fixed(double v) { return __double2ll_rn(v); }
+
+template <typename T, bool DIV, bool SWP, bool SV1>
+__device__ __forceinline__ void scatter_walk_fixed_t(const Walk<T> &w, const GridDev<T> &g, unsigned long long *base,
+                                                     int su, int sv, int sw, T value, T scale)
+{
+    Walker<T, DIV, SWP, SV1> it(w, g, w.k0, su, sv, sw);
+    const T yw = value * w.W;
+    auto f = [&](const SlabSlots<T> &s) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            if (s.ok[j]) atomicAdd(base + s.idx[j], (unsigned long long)to_fixed((yw * s.r[j]) * scale));
+    };
+    walk_all(it, w.k0, w.k1, w.ki0, w.ki1, f);
+}
+
+template <typename T, bool DIV, bool SV1>
+__device__ __forceinline__ void scatter_walk_fixed(const Walk<T> &w, const GridDev<T> &g, unsigned long long *base,
+                                                   int su, int sv, int sw, T value, T scale)
+{
+    if (w.kw >= (T)0) scatter_walk_fixed_t<T, DIV, true, SV1>(w, g, base, su, sv, sw, value, scale);
+    else scatter_walk_fixed_t<T, DIV, false, SV1>(w, g, base, su, sv, sw, value, scale);
+}
+
 // Number of contributions of the ray (the throughput unit).  Uses the
 // reference's exact ratio division, so near-equal crossing ratios order the
 // three-voxel split exactly as the reference does and the count matches it.

@@ -90,3 +90,10 @@ def test_ops_refuse_cpu_tensors(nefct_lib):
     g = _geom()
     with pytest.raises(nb.NefctError, match="CUDA tensor"):
         nb.ops.cb_forward(torch.zeros(g.vol_shape), g)
+
+
+def test_deterministic_workspace_size(nefct_lib):
+    g = _geom().struct()
+    n = 16 ** 3
+    assert nefct_lib.nefct_cb_workspace_bytes(C.byref(g), 0x40) == 256 + 16 * n
+    assert nefct_lib.nefct_cb_workspace_bytes(C.byref(g), 0x40 | 0x20) == 256 + 8 * n

@@ -235,3 +235,29 @@ def test_launch_shapes_give_identical_forward(cuda):
         assert rec["rows"] in (2, 4, 8) and rec["order"] in (0, 1) and len(rec["ms"]) == 6
     finally:
         autotune.apply(saved["rows"], saved["order"])
+
+
+@pytest.mark.parametrize("flags", [0, _lib.LINE_INTEGRAL, _lib.REF_BACKPROJECT, _lib.NO_TRANSPOSE])
+def test_deterministic_transpose_is_bitwise_reproducible(cuda, flags):
+    """NEFCT_DETERMINISTIC: 64-bit fixed-point sums give the same bits on
+    every run, and agree with the float-atomic transpose to float rounding."""
+    g = nb.ConeBeam((48, 40, 36), np.linspace(0, 2 * np.pi, 40, endpoint=False), 140.0, 280.0, 80, 1.2, 60, 1.1,
+                    size=(48.0, 40.0, 36.0))
+    gen = torch.Generator(device=cuda).manual_seed(21)
+    y = torch.randn(g.sino_shape, device=cuda, generator=gen)
+    runs = [ops.cb_backward(y, g, flags | _lib.DETERMINISTIC) for _ in range(3)]
+    for r in runs[1:]:
+        assert torch.equal(r, runs[0])
+    ref = ops.cb_backward(y.double(), g, flags).float()      # FP64 sums as the reference
+    assert_parity(runs[0].cpu().numpy(), ref.cpu().numpy(), rel=1e-6, mabs=1e-5)
+
+
+def test_deterministic_autograd_matches_float_path(cuda):
+    g = nb.ConeBeam((32, 32, 32), np.linspace(0, 2 * np.pi, 30, endpoint=False), 100.0, 200.0, 48, 1.4, 40, 1.4)
+    x = torch.rand(g.vol_shape, device=cuda, generator=torch.Generator(device=cuda).manual_seed(3))
+    grads = []
+    for flags in (0, _lib.DETERMINISTIC):
+        xi = x.clone().requires_grad_()
+        (nb.project(xi, g, flags) ** 2).sum().backward()
+        grads.append(xi.grad)
+    assert_parity(grads[1].cpu().numpy(), grads[0].cpu().numpy(), rel=1e-6, mabs=1e-5)

@@ -101,6 +101,9 @@ typedef struct nefct_cb_geom {
 #define NEFCT_Q5            0x08u /* extra 1/L on y-driven three-voxel middle weights (cpp/siddon :292,:313) */
 #define NEFCT_Q8_INDEX      0x10u /* cylindrical backprojection reads the sinogram at ia + iv*na + ib*na*nb (:830) */
 #define NEFCT_NO_TRANSPOSE  0x20u /* x-driven rays read the x-fastest volume directly: no workspace, slower */
+#define NEFCT_EXACT         0x80u /* classical exact Siddon instead of the reference's slab split: FP64 per-ray
+                                     entry/exit and first crossings, FP32 stepping; exact transpose with the
+                                     same flags.  No counterpart in the reference (its split is quirk Q1) */
 #define NEFCT_DETERMINISTIC 0x40u /* backward: bitwise reproducible sums (64-bit fixed point, see nefct_cb_backward);
                                      the forward is deterministic anyway and ignores it */
 

@@ -22,6 +22,7 @@ Q5 = 0x08
 Q8_INDEX = 0x10
 NO_TRANSPOSE = 0x20
 DETERMINISTIC = 0x40
+EXACT = 0x80
 REF_FORWARD = 0
 REF_BACKPROJECT = TIE_GT | SKIP_SHORT | NO_INV_L2
 LINE_INTEGRAL = NO_INV_L2

@@ -55,7 +55,7 @@ __device__ __forceinline__ void cb_cell(const CBParams<T> &p, int &ia, int &ib, 
     else { ib = blockIdx.y * blockDim.y + threadIdx.y; iv = blockIdx.z; }
 }
 
-template <typename T, bool DIV>
+template <typename T, bool DIV, bool EXACT = false>
 __global__ void __launch_bounds__(256) cb_forward_kernel(const __grid_constant__ CBParams<T> p)
 {
     int ia, ib, iv;
@@ -63,11 +63,11 @@ __global__ void __launch_bounds__(256) cb_forward_kernel(const __grid_constant__
     if (ia >= p.na || ib >= p.nb) return;
     T r[6];
     cb_ray(p, ia, ib, iv, r);
-    const T acc = ray_forward<T, DIV>(p.g, r, p.flags, p.vol, p.volT);
+    const T acc = ray_forward<T, DIV, EXACT>(p.g, r, p.flags, p.vol, p.volT);
     p.out[(size_t)(p.v0 + iv) * p.na * p.nb + (size_t)ib * p.na + ia] = acc;
 }
 
-template <typename T, bool DIV>
+template <typename T, bool DIV, bool EXACT = false>
 __global__ void __launch_bounds__(256) cb_backward_kernel(const __grid_constant__ CBParams<T> p)
 {
     int ia, ib, iv;
@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(256) cb_backward_kernel(const __grid_constant_
     if (y == (T)0) return;
     T r[6];
     cb_ray(p, ia, ib, iv, r);
-    ray_backward<T, DIV>(p.g, r, p.flags, y, p.out, p.outT);
+    ray_backward<T, DIV, EXACT>(p.g, r, p.flags, y, p.out, p.outT);
 }
 
 template <bool DIV>
@@ -237,7 +237,7 @@ template <typename T> static void cb_shape(CBParams<T> &p, int na, int nb, int n
 template <typename T> static bool cubic(const GridDev<T> &g) { return g.dy == (T)1 && g.dz == (T)1; }
 
 static const uint32_t kWalkFlags = NEFCT_TIE_GT | NEFCT_SKIP_SHORT | NEFCT_NO_INV_L2 | NEFCT_Q5 |
-                                   NEFCT_Q8_INDEX | NEFCT_NO_TRANSPOSE | NEFCT_DETERMINISTIC;
+                                   NEFCT_Q8_INDEX | NEFCT_NO_TRANSPOSE | NEFCT_DETERMINISTIC | NEFCT_EXACT;
 
 static nefct_status check_grid(const nefct_grid &g)
 {
@@ -324,7 +324,8 @@ nefct_status cb_forward_launches(const nefct_cb_geom *g, const float *vol, const
         fill_views(p, g, v0, nvc);
         dim3 grid, block;
         cb_shape(p, g->na, g->nb, nvc, grid, block);
-        if (cubic(p.g)) cb_forward_kernel<float, false><<<grid, block, 0, s>>>(p);
+        if (flags & NEFCT_EXACT) cb_forward_kernel<float, false, true><<<grid, block, 0, s>>>(p);
+        else if (cubic(p.g)) cb_forward_kernel<float, false><<<grid, block, 0, s>>>(p);
         else cb_forward_kernel<float, true><<<grid, block, 0, s>>>(p);
         NEFCT_CHECK_LAUNCH("cb_forward_kernel");
     }
@@ -344,7 +345,8 @@ nefct_status cb_backward_launches(const nefct_cb_geom *g, const float *sino, flo
         fill_views(p, g, v0, nvc);
         dim3 grid, block;
         cb_shape(p, g->na, g->nb, nvc, grid, block);
-        if (cubic(p.g)) cb_backward_kernel<float, false><<<grid, block, 0, s>>>(p);
+        if (flags & NEFCT_EXACT) cb_backward_kernel<float, false, true><<<grid, block, 0, s>>>(p);
+        else if (cubic(p.g)) cb_backward_kernel<float, false><<<grid, block, 0, s>>>(p);
         else cb_backward_kernel<float, true><<<grid, block, 0, s>>>(p);
         NEFCT_CHECK_LAUNCH("cb_backward_kernel");
     }
@@ -379,7 +381,8 @@ static nefct_status cb_forward_impl(const nefct_cb_geom *g, const T *vol, T *sin
         fill_views(*p, g, v0, nvc);
         dim3 grid, block;
         cb_shape(*p, g->na, g->nb, nvc, grid, block);
-        if (cubic(p->g)) cb_forward_kernel<T, false><<<grid, block, 0, s>>>(*p);
+        if (flags & NEFCT_EXACT) cb_forward_kernel<T, false, true><<<grid, block, 0, s>>>(*p);
+        else if (cubic(p->g)) cb_forward_kernel<T, false><<<grid, block, 0, s>>>(*p);
         else cb_forward_kernel<T, true><<<grid, block, 0, s>>>(*p);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) { delete p; return cuda_fail(e, "cb_forward_kernel"); }
@@ -414,7 +417,8 @@ size_t cb_fixed_workspace(const nefct_cb_geom *g, uint32_t flags)
 static nefct_status cb_backward_fixed_impl(const nefct_cb_geom *g, const float *sino, float *vol, uint32_t flags,
                                            void *ws, size_t wsb, cudaStream_t s)
 {
-    if (flags & NEFCT_Q5) return fail(NEFCT_ERR_UNSUPPORTED, "NEFCT_Q5 is not available with NEFCT_DETERMINISTIC");
+    if (flags & (NEFCT_Q5 | NEFCT_EXACT))
+        return fail(NEFCT_ERR_UNSUPPORTED, "NEFCT_Q5 and NEFCT_EXACT are not available with NEFCT_DETERMINISTIC");
     if (!(g->src_det > 0.f)) return fail(NEFCT_ERR_INVALID, "deterministic transpose needs src_det > 0");
     const size_t nvox = (size_t)g->grid.nx * g->grid.ny * g->grid.nz;
     const bool tr = !(flags & NEFCT_NO_TRANSPOSE);
@@ -484,7 +488,8 @@ static nefct_status cb_backward_impl(const nefct_cb_geom *g, const T *sino, T *v
         fill_views(*p, g, v0, nvc);
         dim3 grid, block;
         cb_shape(*p, g->na, g->nb, nvc, grid, block);
-        if (cubic(p->g)) cb_backward_kernel<T, false><<<grid, block, 0, s>>>(*p);
+        if (flags & NEFCT_EXACT) cb_backward_kernel<T, false, true><<<grid, block, 0, s>>>(*p);
+        else if (cubic(p->g)) cb_backward_kernel<T, false><<<grid, block, 0, s>>>(*p);
         else cb_backward_kernel<T, true><<<grid, block, 0, s>>>(*p);
         e = cudaGetLastError();
         if (e != cudaSuccess) { delete p; return cuda_fail(e, "cb_backward_kernel"); }
@@ -506,6 +511,8 @@ static nefct_status lor_impl(const nefct_grid *grid, const T *lors, int64_t n, c
     nefct_status st = check_grid(*grid);
     if (st) return st;
     if (n < 0) return fail(NEFCT_ERR_INVALID, "negative LOR count");
+    if (flags & (NEFCT_EXACT | NEFCT_DETERMINISTIC | NEFCT_Q8_INDEX))
+        return fail(NEFCT_ERR_UNSUPPORTED, "the LOR projector takes the walk flags of cpp/siddon only");
     if ((!lors || !src || !dst) && n > 0) return fail(NEFCT_ERR_INVALID, "NULL buffer");
     if (flags & ~kWalkFlags) return fail(NEFCT_ERR_INVALID, "unknown flag bits 0x%x", flags & ~kWalkFlags);
     if (!dst) return fail(NEFCT_ERR_INVALID, "NULL output");
@@ -606,7 +613,8 @@ static nefct_status cb_forward_static_impl(const nefct_cb_geom *g, const float *
         fill_views(p, g, v0, nvc);
         dim3 grid, block;
         cb_shape(p, g->na, g->nb, nvc, grid, block);
-        if (cubic(p.g)) cb_forward_kernel<float, false><<<grid, block, 0, s>>>(p);
+        if (flags & NEFCT_EXACT) cb_forward_kernel<float, false, true><<<grid, block, 0, s>>>(p);
+        else if (cubic(p.g)) cb_forward_kernel<float, false><<<grid, block, 0, s>>>(p);
         else cb_forward_kernel<float, true><<<grid, block, 0, s>>>(p);
         NEFCT_CHECK_LAUNCH("cb_forward_kernel (noalloc)");
     }

@@ -418,11 +418,147 @@ __device__ __forceinline__ unsigned count_walk(const Walk<T> &w, const GridDev<T
     return n;
 }
 
+// ---------------- exact Siddon (NEFCT_EXACT) ----------------
+//
+// Classical plane-crossing traversal (Siddon 1985; incremental form of
+// Jacobs et al. 1998): the segment p1 -> p2 is clipped to the grid box and
+// split at every x, y and z plane it crosses; each piece contributes its
+// exact length times the voxel value.  FP64 is used only for the per-ray
+// set-up -- entry/exit parameters alpha_min/alpha_max, the first voxel and
+// the first plane crossings -- where FP32 cancellation would drop or
+// duplicate pieces at grazing angles; the stepping runs in T (FP32 for the
+// float build) from those values.  Weights: length (physical units) times
+// 1/L^2 in x-pitch voxel units unless NEFCT_NO_INV_L2, as in the default
+// walk.  The loop is bounded by nx + ny + nz + 4 steps.
+template <typename T> struct ExactRay {
+    T alpha, amax, ax, ay, az, dax, day, daz, scale;
+    int i, j, k, di, dj, dk;
+    bool xdom;                // |dx| >= |dy|: gather from the y-fastest copy
+};
+
+template <typename T>
+__device__ __forceinline__ bool exact_setup(const GridDev<T> &g, const T *r, uint32_t flags, ExactRay<T> &e)
+{
+    const int n[3] = {g.nx, g.ny, g.nz};
+    const double dx_ = (double)g.dx_;
+    const double pitch[3] = {dx_, (double)g.dy * dx_, (double)g.dz * dx_};
+    const double c[3] = {(double)g.cx, (double)g.cy, (double)g.cz};
+    double p1[3], d[3], lo[3];
+    double amin = 0.0, amax = 1.0;
+    for (int a = 0; a < 3; ++a) {
+        p1[a] = (double)r[a];
+        d[a] = (double)r[a + 3] - p1[a];
+        lo[a] = c[a] - 0.5 * n[a] * pitch[a];
+        if (d[a] != 0.0) {
+            double a0 = (lo[a] - p1[a]) / d[a], a1 = (lo[a] + n[a] * pitch[a] - p1[a]) / d[a];
+            if (a0 > a1) { const double t = a0; a0 = a1; a1 = t; }
+            amin = fmax(amin, a0);
+            amax = fmin(amax, a1);
+        } else if (p1[a] < lo[a] || p1[a] >= lo[a] + n[a] * pitch[a]) {
+            return false;
+        }
+    }
+    if (!(amax > amin)) return false;
+    const double L = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    if ((flags & NEFCT_SKIP_SHORT) && sqrt(d[0] * d[0] + d[1] * d[1]) / dx_ < 10.0) return false;
+    int idx[3], step[3];
+    double anext[3], dal[3];
+    // first voxel: the one containing the middle of the first piece
+    double first = amax;
+    for (int a = 0; a < 3; ++a) {
+        if (d[a] == 0.0) continue;
+        const double s = (floor((p1[a] + amin * d[a] - lo[a]) / pitch[a]) + (d[a] > 0 ? 1.0 : 0.0)) * pitch[a] + lo[a];
+        double ap = (s - p1[a]) / d[a];
+        if (ap <= amin) ap += pitch[a] / fabs(d[a]);
+        first = fmin(first, ap);
+    }
+    const double am = 0.5 * (amin + first);
+    for (int a = 0; a < 3; ++a) {
+        int i = (int)floor((p1[a] + am * d[a] - lo[a]) / pitch[a]);
+        i = max(0, min(n[a] - 1, i));
+        idx[a] = i;
+        if (d[a] > 0.0) {
+            step[a] = 1;
+            anext[a] = (lo[a] + (i + 1) * pitch[a] - p1[a]) / d[a];
+            dal[a] = pitch[a] / d[a];
+        } else if (d[a] < 0.0) {
+            step[a] = -1;
+            anext[a] = (lo[a] + i * pitch[a] - p1[a]) / d[a];
+            dal[a] = -pitch[a] / d[a];
+        } else {
+            step[a] = 0;
+            anext[a] = 1e30;
+            dal[a] = 0.0;
+        }
+    }
+    double scale = L;                       // parameter length -> physical length
+    if (!(flags & NEFCT_NO_INV_L2)) scale *= (dx_ * dx_) / (L * L);
+    e.alpha = (T)amin; e.amax = (T)amax;
+    e.ax = (T)anext[0]; e.ay = (T)anext[1]; e.az = (T)anext[2];
+    e.dax = (T)dal[0]; e.day = (T)dal[1]; e.daz = (T)dal[2];
+    e.i = idx[0]; e.j = idx[1]; e.k = idx[2];
+    e.di = step[0]; e.dj = step[1]; e.dk = step[2];
+    e.scale = (T)scale;
+    e.xdom = fabs(d[0]) >= fabs(d[1]);
+    return true;
+}
+
+// Visits (voxel index, piece length in parameter units) along the ray.
+template <typename T, class Fn>
+__device__ __forceinline__ void exact_walk(const GridDev<T> &g, ExactRay<T> e, int su, int sv, int sw, Fn &f)
+{
+    const int limit = g.nx + g.ny + g.nz + 4;
+    for (int it = 0; it < limit; ++it) {
+        if (!(e.alpha < e.amax) || (unsigned)e.i >= (unsigned)g.nx || (unsigned)e.j >= (unsigned)g.ny ||
+            (unsigned)e.k >= (unsigned)g.nz)
+            break;
+        const T an = fmin(e.ax, fmin(e.ay, e.az));
+        const T aend = fmin(an, e.amax);
+        const T len = aend - e.alpha;
+        // (u, v) layout: x-dominant rays use the y-fastest copy (su = ny, sv = 1 with u = x)
+        const int id = e.xdom ? e.i * su + e.j * sv + e.k * sw : e.j * su + e.i * sv + e.k * sw;
+        if (len > (T)0) f(id, len);
+        e.alpha = aend;
+        if (an == e.ax) { e.i += e.di; e.ax += e.dax; }
+        else if (an == e.ay) { e.j += e.dj; e.ay += e.day; }
+        else { e.k += e.dk; e.az += e.daz; }
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ T exact_forward(const GridDev<T> &g, const T *r, uint32_t flags, const T *vol, const T *volT)
+{
+    ExactRay<T> e;
+    if (!exact_setup(g, r, flags, e)) return (T)0;
+    T acc = (T)0;
+    auto f = [&](int id, T len) { acc += __ldg(((e.xdom && volT) ? volT : vol) + id) * len; };
+    const int sw = g.nx * g.ny;
+    if (e.xdom && volT) exact_walk(g, e, g.ny, 1, sw, f);
+    else if (e.xdom) exact_walk(g, e, 1, g.nx, sw, f);
+    else exact_walk(g, e, g.nx, 1, sw, f);
+    return acc * e.scale;
+}
+
+template <typename T>
+__device__ __forceinline__ void exact_backward(const GridDev<T> &g, const T *r, uint32_t flags, T y, T *out, T *outT)
+{
+    ExactRay<T> e;
+    if (!exact_setup(g, r, flags, e)) return;
+    const T ys = y * e.scale;
+    T *base = (e.xdom && outT) ? outT : out;
+    auto f = [&](int id, T len) { atomicAdd(base + id, ys * len); };
+    const int sw = g.nx * g.ny;
+    if (e.xdom && outT) exact_walk(g, e, g.ny, 1, sw, f);
+    else if (e.xdom) exact_walk(g, e, 1, g.nx, sw, f);
+    else exact_walk(g, e, g.nx, 1, sw, f);
+}
+
 // Forward value of one ray: gathers x-driven rays from the y-fastest copy
 // volT when there is one, everything else from the x-fastest volume.
-template <typename T, bool DIV>
+template <typename T, bool DIV, bool EXACT = false>
 __device__ __forceinline__ T ray_forward(const GridDev<T> &g, const T *r, uint32_t flags, const T *vol, const T *volT)
 {
+    if (EXACT) return exact_forward(g, r, flags, vol, volT);
     Walk<T> w;
     if (!setup_walk(g, r, flags, w)) return (T)0;
     const int sw = g.nx * g.ny;
@@ -433,9 +569,13 @@ __device__ __forceinline__ T ray_forward(const GridDev<T> &g, const T *r, uint32
 
 // Transpose contribution of one ray with value y: x-driven rays reduce into
 // the y-fastest accumulator outT when there is one.
-template <typename T, bool DIV>
+template <typename T, bool DIV, bool EXACT = false>
 __device__ __forceinline__ void ray_backward(const GridDev<T> &g, const T *r, uint32_t flags, T y, T *out, T *outT)
 {
+    if (EXACT) {
+        exact_backward(g, r, flags, y, out, outT);
+        return;
+    }
     Walk<T> w;
     if (!setup_walk(g, r, flags, w)) return;
     const int sw = g.nx * g.ny;

@@ -303,6 +303,43 @@ def run_gpu(args):
                                                           else "view outermost",
                                                           "autotune_ms": tuned["ms"]}}
 
+    # FDK of this scanner (configuration 2): line-integral projections of the
+    # phantom, cosine weight + ramp filter + weighted voxel-driven backprojection
+    from nefct_b200 import recon
+    fdk = {}
+    lines = ops.cb_forward(vol, geom, nb._lib.LINE_INTEGRAL)
+    for win in ("ram-lak", "shepp-logan"):
+        recon.fdk(lines, geom, win)
+        ef = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ef[0].record()
+        filt = ops.fdk_filter(lines, geom, win)
+        ef[1].record()
+        rec = ops.fdk_backproject(filt, geom)
+        ef[2].record()
+        torch.cuda.synchronize()
+        t_f, t_b = ef[0].elapsed_time(ef[1]) / 1e3, ef[1].elapsed_time(ef[2]) / 1e3
+        c = slice(n // 4, 3 * n // 4)
+        err = float((rec[c, c, c] - vol[c, c, c]).norm() / vol[c, c, c].norm())
+        fdk[win] = {"filter_ms": 1e3 * t_f, "backproject_ms": 1e3 * t_b,
+                    "voxels_per_s": n ** 3 / (t_f + t_b), "voxel_views_per_s": n ** 3 * CFG["nv"] / t_b,
+                    "central_rel_error_vs_phantom": err}
+    # short scan 180 deg + fan with Parker weights (views spaced like the full scan)
+    fan = 2 * np.degrees(np.arctan(CFG["na"] * CFG["pixel"] / 2 / CFG["src_det"]))
+    step = 360.0 / CFG["nv"]
+    nss = int(np.ceil((180 + fan) / step)) + 1
+    gss = nb.ConeBeam((n, n, n), np.deg2rad(np.arange(nss) * step - fan / 2), CFG["src_iso"], CFG["src_det"],
+                      CFG["na"], CFG["pixel"], CFG["nb"], CFG["pixel"], size=(n * CFG["voxel"],) * 3)
+    lss = ops.cb_forward(vol, gss, nb._lib.LINE_INTEGRAL)
+    best = None
+    for d in (1, -1):
+        rec = recon.fdk(lss, gss, "ram-lak", d)
+        c = slice(n // 4, 3 * n // 4)
+        err = float((rec[c, c, c] - vol[c, c, c]).norm() / vol[c, c, c].norm())
+        best = (err, d) if best is None or err < best[0] else best
+    fdk["short_scan_parker"] = {"views": nss, "dir": best[1], "central_rel_error_vs_phantom": best[0]}
+    del lines, filt, rec, lss
+    extras["fdk"] = fdk
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         v, kind, cores, sample = cpu_sample(2, 3)
@@ -416,6 +453,110 @@ def run_batched(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------- differentiable projector at 512^3 (configuration 3) ----------------
+
+def run_diff512(args):
+    """512^3 phantom (50 ellipsoids, seed 3), 720 views, 1024x768 at 1 mm,
+    source-axis 700 / source-detector 1400 mm, b = A x + 1 % noise (seed 33):
+    forward + adjoint intersections/s through autograd, and 20 SIRT
+    iterations."""
+    import torch
+    import nefct_b200 as nb
+    from nefct_b200 import ops, recon
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    n, nv = int(512 * args.scale), int(720 * args.scale)
+    na, nbr = int(1024 * args.scale), int(768 * args.scale)
+    g = nb.ConeBeam((n, n, n), np.linspace(0, 2 * np.pi, nv, endpoint=False), 700.0, 1400.0, na, 1.0, nbr, 1.0,
+                    size=(float(n),) * 3)
+    x_true = nb.ellipsoid_phantom(n, nb.random_ellipsoids(50, 3), device=dev).permute(2, 1, 0).contiguous()
+    flags = nb._lib.LINE_INTEGRAL
+    b = ops.cb_forward(x_true, g, flags)
+    gen = torch.Generator(device=dev).manual_seed(33)
+    b += 0.01 * float(b.max()) * torch.randn(b.shape, device=dev, generator=gen)
+    inter = ops.cb_count_intersections(g, flags, dev)
+    x = torch.zeros_like(x_true, requires_grad=True)
+
+    def fb():
+        loss = ((nb.project(x, g, flags) - b) ** 2).sum()
+        loss.backward()
+        return loss
+    for _ in range(args.warmup):
+        fb()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        fb()
+    e1.record()
+    torch.cuda.synchronize()
+    t_fb = e0.elapsed_time(e1) / 1e3 / args.steps
+    # 20 SIRT iterations
+    e0.record()
+    rec = recon.sirt(b, g, 20, flags)
+    e1.record()
+    torch.cuda.synchronize()
+    t_sirt = e0.elapsed_time(e1) / 1e3
+    err = float((rec - x_true).norm() / x_true.norm())
+    line = {"metric": "ray-voxel intersections/s (autograd forward + adjoint, 512^3 differentiable projector)",
+            "value": 2 * inter / t_fb, "unit": "intersections/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_fb, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ellipsoid phantom + 1 % noise)",
+            "config": {"workload": f"{n}^3 @1mm, 50 ellipsoids, {nv} views, {na}x{nbr} @1mm, SID 700 / SDD 1400 mm"},
+            "extras": {"intersections_per_direction": inter, "sirt_20_iterations_s": t_sirt,
+                       "sirt_rel_error_vs_phantom": err}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------- motion-compensated 4D through the warp (configuration 5) ----------------
+
+def run_motion4d(args):
+    """256^3 reference volume, 10 phases x 72 views, 512x384, per-phase
+    displacement fields (4 seeded sinusoids, <= 5 voxels): warp then project,
+    gradients w.r.t. the volume and every field (autograd)."""
+    import torch
+    import nefct_b200 as nb
+    from nefct_b200 import ops, recon
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    n = 256
+    phases, per = 10, 72
+    ang = np.linspace(0, 2 * np.pi, phases * per, endpoint=False)
+    geoms = [nb.ConeBeam((n, n, n), ang[p::phases], 600.0, 1200.0, 512, 1.2, 384, 1.2, size=(float(n),) * 3)
+             for p in range(phases)]
+    ref = nb.ellipsoid_phantom(n, nb.random_ellipsoids(30, 5), device=dev).permute(2, 1, 0).contiguous()
+    rng = np.random.default_rng(5)
+    fields = [recon.sinusoid_field(ref.shape, 5.0, rng, device=dev) for _ in range(phases)]
+    targets = [ops.cb_forward(ops.warp_forward(ref, *m), g) for m, g in zip(fields, geoms)]
+    inter = sum(ops.cb_count_intersections(g, 0, dev) for g in geoms)
+    x = ref.clone().mul_(0.9).requires_grad_()
+    ms = [[c.clone().requires_grad_() for c in m] for m in fields]
+
+    def fb():
+        sinos = recon.motion_project(x, ms, geoms)
+        loss = sum(((s_ - t) ** 2).sum() for s_, t in zip(sinos, targets))
+        loss.backward()
+    for _ in range(args.warmup):
+        fb()
+    torch.cuda.synchronize()
+    peak = torch.cuda.max_memory_allocated(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        fb()
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / args.steps
+    line = {"metric": "ray-voxel intersections/s (4D warp + forward + adjoint with image and field gradients)",
+            "value": 2 * inter / t, "unit": "intersections/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom and sinusoid fields)",
+            "config": {"workload": f"{n}^3, {phases} phases x {per} views, 512x384 @1.2mm, fields 3x{n}^3 per phase"},
+            "extras": {"intersections_per_direction": inter, "voxels_warped_per_step": phases * n ** 3,
+                       "peak_allocated_bytes": peak}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -426,7 +567,7 @@ def main():
     ap.add_argument("--views", type=int, default=360, help="views of the scan (360 = the workload; fewer only for profiling)")
     ap.add_argument("--rows", type=int, default=0, help="fix the detector rows per CTA instead of autotuning")
     ap.add_argument("--order", type=int, default=1, help="with --rows: 0 row bands outermost, 1 views outermost")
-    ap.add_argument("--workload", default="fdk-scanner", choices=["fdk-scanner", "batched"],
+    ap.add_argument("--workload", default="fdk-scanner", choices=["fdk-scanner", "batched", "diff512", "motion4d"],
                     help="batched: the uneven-problems configuration (its own JSON line)")
     ap.add_argument("--problems", type=int, default=64)
     ap.add_argument("--scale", type=float, default=1.0, help="batched: scale of volume edges and detector sizes")
@@ -436,6 +577,10 @@ def main():
         run_reference(args)
     elif args.workload == "batched":
         run_batched(args)
+    elif args.workload == "diff512":
+        run_diff512(args)
+    elif args.workload == "motion4d":
+        run_motion4d(args)
     else:
         run_gpu(args)
 

@@ -268,6 +268,13 @@ nefct_status nefct_warp_adjoint(const float *gout, const float *mx, const float 
 nefct_status nefct_warp_grad_dvf(const float *img, const float *mx, const float *my, const float *mz,
                                  const float *gout, int32_t nx, int32_t ny, int32_t nz,
                                  float *gmx, float *gmy, float *gmz, void *stream);
+/* Inverse of a displacement field by `iters` fixed-point passes (the
+ * reference uses 30): replaces DeformInvert (nefct/cc/deform/deform_tex.cc:24,
+ * deform_tex.cu.cc:78-99).  Fields are sampled trilinearly with
+ * clamp-to-edge addressing in FP32 (the reference samples a linear-filtered
+ * texture, whose weights carry 8 fractional bits). */
+nefct_status nefct_warp_invert(const float *mx, const float *my, const float *mz, int32_t nx, int32_t ny, int32_t nz,
+                               int32_t iters, float *ix, float *iy, float *iz, void *stream);
 nefct_status nefct_warp_forward_f64(const double *img, const double *mx, const double *my, const double *mz,
                                     int32_t nx, int32_t ny, int32_t nz, double *out, void *stream);
 nefct_status nefct_warp_adjoint_f64(const double *gout, const double *mx, const double *my, const double *mz,

@@ -119,6 +119,48 @@ __global__ void __launch_bounds__(256) warp_grad_dvf_kernel(const T *__restrict_
     gmz[id] = gz;
 }
 
+
+// Displacement-field inversion of nefct/cc/deform/deform_tex.cu.cc:78-99:
+// starting from 0, `iters` Gauss-Seidel fixed-point passes
+//   x <- -mx(p + (x, y, z)),  y <- -my(...),  z <- -mz(...)
+// sampled trilinearly with clamp-to-edge addressing (the reference samples a
+// linear-filtered, clamp-addressed texture at texel centres; hardware
+// filtering keeps 8 fractional bits of the weights, this samples in FP32).
+__device__ __forceinline__ float clamp_lerp3(const float *__restrict__ m, float px, float py, float pz, int nx, int ny,
+                                             int nz)
+{
+    const float fx = floorf(px), fy = floorf(py), fz = floorf(pz);
+    const float ax = px - fx, ay = py - fy, az = pz - fz;
+    const int x0 = min(max((int)fx, 0), nx - 1), x1 = min(max((int)fx + 1, 0), nx - 1);
+    const int y0 = min(max((int)fy, 0), ny - 1), y1 = min(max((int)fy + 1, 0), ny - 1);
+    const int z0 = min(max((int)fz, 0), nz - 1), z1 = min(max((int)fz + 1, 0), nz - 1);
+    const size_t sy = nx, sz = (size_t)nx * ny;
+    const float c00 = __ldg(m + x0 + y0 * sy + z0 * sz) * (1.f - ax) + __ldg(m + x1 + y0 * sy + z0 * sz) * ax;
+    const float c10 = __ldg(m + x0 + y1 * sy + z0 * sz) * (1.f - ax) + __ldg(m + x1 + y1 * sy + z0 * sz) * ax;
+    const float c01 = __ldg(m + x0 + y0 * sy + z1 * sz) * (1.f - ax) + __ldg(m + x1 + y0 * sy + z1 * sz) * ax;
+    const float c11 = __ldg(m + x0 + y1 * sy + z1 * sz) * (1.f - ax) + __ldg(m + x1 + y1 * sy + z1 * sz) * ax;
+    const float c0 = c00 * (1.f - ay) + c10 * ay, c1 = c01 * (1.f - ay) + c11 * ay;
+    return c0 * (1.f - az) + c1 * az;
+}
+
+__global__ void __launch_bounds__(256) warp_invert_kernel(const float *__restrict__ mx, const float *__restrict__ my,
+                                                          const float *__restrict__ mz, int nx, int ny, int nz,
+                                                          int iters, float *ix, float *iy, float *iz)
+{
+    const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+    if (x >= nx || y >= ny) return;
+    float u = 0.f, v = 0.f, w = 0.f;
+    for (int it = 0; it < iters; ++it) {
+        u = -clamp_lerp3(mx, x + u, y + v, z + w, nx, ny, nz);
+        v = -clamp_lerp3(my, x + u, y + v, z + w, nx, ny, nz);
+        w = -clamp_lerp3(mz, x + u, y + v, z + w, nx, ny, nz);
+    }
+    const size_t id = x + (size_t)y * nx + (size_t)z * nx * ny;
+    ix[id] = u;
+    iy[id] = v;
+    iz[id] = w;
+}
+
 static nefct_status check_warp(int nx, int ny, int nz)
 {
     if (nx < 1 || ny < 1 || nz < 1) return fail(NEFCT_ERR_INVALID, "warp grid must be >= 1 (got %d x %d x %d)", nx, ny, nz);
@@ -207,6 +249,19 @@ nefct_status nefct_warp_grad_dvf_f64(const double *img, const double *mx, const 
                                      double *gmy, double *gmz, void *stream)
 {
     return warp_grad_impl<double>(img, mx, my, mz, gout, nx, ny, nz, gmx, gmy, gmz, (cudaStream_t)stream);
+}
+
+nefct_status nefct_warp_invert(const float *mx, const float *my, const float *mz, int32_t nx, int32_t ny, int32_t nz,
+                               int32_t iters, float *ix, float *iy, float *iz, void *stream)
+{
+    nefct_status st = check_warp(nx, ny, nz);
+    if (st) return st;
+    if (!mx || !my || !mz || !ix || !iy || !iz) return fail(NEFCT_ERR_INVALID, "NULL buffer");
+    if (iters < 0 || iters > 10000) return fail(NEFCT_ERR_INVALID, "iters must be in [0, 10000]");
+    warp_invert_kernel<<<dim3((nx + 31) / 32, (ny + 7) / 8, nz), dim3(32, 8), 0, (cudaStream_t)stream>>>(
+        mx, my, mz, nx, ny, nz, iters, ix, iy, iz);
+    NEFCT_CHECK_LAUNCH("warp_invert_kernel");
+    return NEFCT_OK;
 }
 
 }  // extern "C"

@@ -26,7 +26,7 @@ from ._lib import NefctError
 
 __all__ = ["ConeBeam", "cb_forward", "cb_backward", "cb_count_intersections", "lor_forward",
            "lor_backward", "fdk_filter", "fdk_backproject", "warp_forward", "warp_adjoint",
-           "warp_grad_dvf", "project", "backproject", "warp", "NefctError"]
+           "warp_grad_dvf", "warp_invert", "project", "backproject", "warp", "NefctError"]
 
 
 @dataclass(eq=False)
@@ -280,6 +280,19 @@ def warp_grad_dvf(img, mx, my, mz, gout):
                   mz.data_ptr(), gout.data_ptr(), nx, ny, nz, gx.data_ptr(), gy.data_ptr(), gz.data_ptr(),
                   _stream(img))
     return gx, gy, gz
+
+
+def warp_invert(mx, my, mz, iters: int = 30):
+    """Inverse displacement field (DeformInvert, deform_tex.cu.cc:78-99)."""
+    _check_warp(mx, my, mz)
+    if mx.dtype != torch.float32:
+        raise NefctError(_lib.ERR_INVALID, "warp_invert is float32")
+    nz, ny, nx = mx.shape
+    ix, iy, iz = torch.empty_like(mx), torch.empty_like(mx), torch.empty_like(mx)
+    with torch.cuda.device(mx.device):
+        _lib.call("nefct_warp_invert", mx.data_ptr(), my.data_ptr(), mz.data_ptr(), nx, ny, nz, int(iters),
+                  ix.data_ptr(), iy.data_ptr(), iz.data_ptr(), _stream(mx))
+    return ix, iy, iz
 
 
 # ---------------- autograd ----------------

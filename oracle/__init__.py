@@ -218,6 +218,16 @@ def deform(img, mx, my, mz, f64=False):
     return out
 
 
+def warp_invert(mx, my, mz, iters=30):
+    L = lib()
+    mx, my, mz = _f32(mx), _f32(my), _f32(mz)
+    nz, ny, nx = mx.shape
+    out = [np.zeros_like(mx) for _ in range(3)]
+    L.or_warp_invert_f32(_p(mx), _p(my), _p(mz), C.c_int(nx), C.c_int(ny), C.c_int(nz), C.c_int(iters),
+                         *[_p(o) for o in out])
+    return out
+
+
 # ---------------- the reference itself, compiled for the host ----------------
 
 def ref_cb_forward(g: Grid, vol, angles, SID, SAD, na, da, ai, nb, db, bi, *, cyl=False, f64=False):

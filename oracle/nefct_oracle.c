@@ -242,3 +242,43 @@ void or_deform_f64(const double *img, const double *mx, const double *my, const 
 {
     DEFORM_BODY(double, floor)
 }
+
+/* ---- displacement-field inversion, nefct/cc/deform/deform_tex.cu.cc:78-99 ----
+ * Fixed-point passes x <- -mx(p + d), y <- -my(p + d), z <- -mz(p + d) from
+ * d = 0, trilinear sampling with clamp-to-edge addressing (the reference
+ * samples a clamp-addressed linear-filtered texture at texel centres). */
+static float clamp_lerp3_f32(const float *m, float px, float py, float pz, int nx, int ny, int nz)
+{
+    const float fx = floorf(px), fy = floorf(py), fz = floorf(pz);
+    const float ax = px - fx, ay = py - fy, az = pz - fz;
+#define CL(v, n) ((v) < 0 ? 0 : ((v) > (n) - 1 ? (n) - 1 : (v)))
+    const int x0 = CL((int)fx, nx), x1 = CL((int)fx + 1, nx);
+    const int y0 = CL((int)fy, ny), y1 = CL((int)fy + 1, ny);
+    const int z0 = CL((int)fz, nz), z1 = CL((int)fz + 1, nz);
+#undef CL
+    const long long sy = nx, sz = (long long)nx * ny;
+    const float c00 = m[x0 + y0 * sy + z0 * sz] * (1.f - ax) + m[x1 + y0 * sy + z0 * sz] * ax;
+    const float c10 = m[x0 + y1 * sy + z0 * sz] * (1.f - ax) + m[x1 + y1 * sy + z0 * sz] * ax;
+    const float c01 = m[x0 + y0 * sy + z1 * sz] * (1.f - ax) + m[x1 + y0 * sy + z1 * sz] * ax;
+    const float c11 = m[x0 + y1 * sy + z1 * sz] * (1.f - ax) + m[x1 + y1 * sy + z1 * sz] * ax;
+    const float c0 = c00 * (1.f - ay) + c10 * ay, c1 = c01 * (1.f - ay) + c11 * ay;
+    return c0 * (1.f - az) + c1 * az;
+}
+
+void or_warp_invert_f32(const float *mx, const float *my, const float *mz, int nx, int ny, int nz, int iters,
+                        float *ix, float *iy, float *iz)
+{
+    #pragma omp parallel for collapse(2) schedule(static)
+    for (int z = 0; z < nz; ++z)
+        for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x) {
+                float u = 0.f, v = 0.f, w = 0.f;
+                for (int it = 0; it < iters; ++it) {
+                    u = -clamp_lerp3_f32(mx, x + u, y + v, z + w, nx, ny, nz);
+                    v = -clamp_lerp3_f32(my, x + u, y + v, z + w, nx, ny, nz);
+                    w = -clamp_lerp3_f32(mz, x + u, y + v, z + w, nx, ny, nz);
+                }
+                const long long id = x + (long long)y * nx + (long long)z * nx * ny;
+                ix[id] = u; iy[id] = v; iz[id] = w;
+            }
+}

@@ -85,6 +85,11 @@ void or_deform_f32(const float *img, const float *mx, const float *my, const flo
 void or_deform_f64(const double *img, const double *mx, const double *my, const double *mz,
                    int nx, int ny, int nz, double *out);
 
+/* Displacement-field inversion of nefct/cc/deform/deform_tex.cu.cc:78-99
+ * (FP32 trilinear, clamp-to-edge, Gauss-Seidel fixed point). */
+void or_warp_invert_f32(const float *mx, const float *my, const float *mz, int nx, int ny, int nz, int iters,
+                        float *ix, float *iy, float *iz);
+
 #ifdef __cplusplus
 }
 #endif

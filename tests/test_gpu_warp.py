@@ -74,3 +74,13 @@ def test_warp_then_project_autograd(cuda):
 
     fd = (f(h) - f(-h)) / (2 * h)
     assert abs(fd - an) <= 1e-5 * abs(an)
+
+
+def test_warp_invert_vs_oracle(cuda, oracle_lib):
+    rng = np.random.default_rng(12)
+    shape = (18, 20, 22)
+    m = [rng.uniform(-1.5, 1.5, shape).astype(np.float32) for _ in range(3)]
+    out = [t.cpu().numpy() for t in ops.warp_invert(*[torch.from_numpy(a).to(cuda) for a in m], iters=30)]
+    ref = oracle_lib.warp_invert(*m, iters=30)
+    for o, r in zip(out, ref):
+        assert_parity(o, r, rel=1e-5, mabs=1e-4)

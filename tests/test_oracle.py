@@ -110,3 +110,20 @@ def test_reference_discretisation_vs_exact_siddon(oracle_lib, golden):
     ref = golden[f"{name}/fwd64"]
     rel = np.linalg.norm(ref - ex) / np.linalg.norm(ex)
     assert 1e-4 < rel < 3e-2
+
+
+def test_warp_invert_oracle_composes_to_identity(oracle_lib):
+    """The fixed-point inverse of a smooth small field satisfies
+    inv(p) = -m(p + inv(p)) in the interior."""
+    n = 24
+    z, y, x = np.meshgrid(*[np.linspace(0, 1, n)] * 3, indexing="ij")
+    m = [1.2 * np.sin(2 * np.pi * (x + 0.3 * y)), 0.8 * np.cos(2 * np.pi * z), 0.6 * np.sin(2 * np.pi * y)]
+    m = [a.astype(np.float32) for a in m]
+    inv = oracle_lib.warp_invert(*m, iters=30)
+    # m(p + inv(p)) + inv(p) ~ 0 in the interior (the fixed point of the iteration)
+    from scipy.ndimage import map_coordinates
+    c = slice(4, n - 4)
+    pz, py, px = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    pos = [pz + inv[2], py + inv[1], px + inv[0]]
+    res = [map_coordinates(m[k], pos, order=1, mode="nearest") + inv[k] for k in range(3)]
+    assert max(np.abs(r[c, c, c]).max() for r in res) < 1e-3

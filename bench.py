@@ -235,8 +235,8 @@ def run_gpu(args):
 
     from nefct_b200 import autotune
     if args.rows:
-        autotune.apply(args.rows, args.order)                          # fixed launch shape (profiling)
-        tuned = {"rows": args.rows, "order": args.order, "ms": None}
+        autotune.apply(args.rows, args.order, args.walk)               # fixed launch shape (profiling)
+        tuned = {"rows": args.rows, "order": args.order, "walk": args.walk, "ms": None}
     else:
         tuned = autotune.tune_cone_beam(geom, 0, dev, use_cache=False)  # untimed launch-shape choice
     for _ in range(args.warmup):
@@ -301,6 +301,10 @@ def run_gpu(args):
               "wall_s_timed_loop": wall, "launch_shape": {"rows_per_cta": tuned["rows"],
                                                           "grid_order": "row-band outermost" if tuned["order"] == 0
                                                           else "view outermost",
+                                                          "walk": {"forward": "column warps" if tuned["walk"] & 1
+                                                                   else "thread per ray",
+                                                                   "adjoint": "column warps" if tuned["walk"] & 2
+                                                                   else "thread per ray"},
                                                           "autotune_ms": tuned["ms"]}}
 
     # FDK of this scanner (configuration 2): line-integral projections of the
@@ -567,6 +571,8 @@ def main():
     ap.add_argument("--views", type=int, default=360, help="views of the scan (360 = the workload; fewer only for profiling)")
     ap.add_argument("--rows", type=int, default=0, help="fix the detector rows per CTA instead of autotuning")
     ap.add_argument("--order", type=int, default=1, help="with --rows: 0 row bands outermost, 1 views outermost")
+    ap.add_argument("--walk", type=int, default=3,
+                    help="with --rows: column warps for the forward (bit 0) / adjoint (bit 1), else thread per ray")
     ap.add_argument("--workload", default="fdk-scanner", choices=["fdk-scanner", "batched", "diff512", "motion4d"],
                     help="batched: the uneven-problems configuration (its own JSON line)")
     ap.add_argument("--problems", type=int, default=64)

@@ -43,16 +43,23 @@ const char *nefct_last_error(void);
 
 /* Process-wide launch tuning used by the autotuner (nefct_b200/autotune.py).
  * No counterpart in the reference (its launch shapes are constants,
- * siddon.cu.cc:8-10).  Every value runs the same per-ray arithmetic: the
- * forward's output is bitwise independent of it; the transpose sums with
- * atomics, whose order is not fixed under any setting.
+ * siddon.cu.cc:8-10).  Every value runs the same per-ray arithmetic in the
+ * same order; the transpose sums with atomics, whose order is not fixed
+ * under any setting.
  *   NEFCT_TUNE_CB_ROWS   detector rows per CTA of the cone-beam Siddon
  *                        kernels (1, 2, 4, 8; 32 columns per row); default 8
  *   NEFCT_TUNE_CB_ORDER  0: row bands outermost (default; keeps the volume
- *                        slab of the rows in flight in L2), 1: views outermost */
+ *                        slab of the rows in flight in L2), 1: views outermost
+ *   NEFCT_TUNE_CB_WALK   bit 0 forward, bit 1 transpose: column warps (FP32
+ *                        slab walk with a workspace) -- each warp walks 32
+ *                        rows of one detector column, which share their
+ *                        transverse walk, over a z-fastest copy of the volume,
+ *                        and NEFCT_TUNE_CB_ROWS counts columns per CTA; a
+ *                        clear bit: one thread per ray.  Default 3 */
 #define NEFCT_TUNE_CB_ROWS  0
 #define NEFCT_TUNE_CB_ORDER 1
-#define NEFCT_TUNE_COUNT    2
+#define NEFCT_TUNE_CB_WALK  2
+#define NEFCT_TUNE_COUNT    3
 nefct_status nefct_tune_set(int32_t key, int32_t value);
 int32_t nefct_tune_get(int32_t key);
 

@@ -1,0 +1,237 @@
+// Cone-beam Siddon kernels (forward and transpose) and their launch
+// dispatch, shared by cb_forward.cu and cb_backward.cu, which instantiate
+// them (one direction per translation unit), and siddon.cu (host side).
+//
+// Two walks, chosen per direction by NEFCT_TUNE_CB_WALK:
+//  * thread per ray (cb_forward_kernel / cb_backward_kernel): 32 adjacent
+//    detector columns x blockDim.y rows per CTA, each warp 32 neighbouring
+//    columns of one row; volume x-fastest plus a y-fastest copy for x-driven
+//    rays;
+//  * column warps (cb_colwarp_kernel, FP32): each warp 32 consecutive rows
+//    of one column, blockDim.y columns per CTA, over a z-fastest copy of the
+//    volume (colwarp.cuh).
+// The grid runs (column tile, view, row band) with the row band slowest, or
+// (column tile, row band, view).  Per-view cos/sin/z-offset ride in the
+// kernel parameters.
+#pragma once
+
+#include <type_traits>
+
+#include "colwarp.cuh"
+
+namespace nefct {
+
+template <typename T> struct CBParams {
+    GridDev<T> g;
+    int na, nb, nvc, v0, nv_total;
+    RayGeom<T> rg;
+    int band_major;
+    uint32_t flags;
+    const T *vol;        // x-fastest volume (forward source)
+    const T *volT;       // y-fastest copy for x-driven rays (thread walk) or z-fastest copy (column warps)
+    const T *sino;       // backward source, full sinogram
+    T *out;              // forward: full sinogram; backward: x-fastest volume
+    T *outT;             // backward: y-fastest or z-fastest accumulator, or nullptr
+    unsigned long long *fix, *fixT;   // deterministic backward: integer accumulators
+    const float *fix_scale;           // deterministic backward: power-of-two scale (device)
+    unsigned long long *count;
+    ViewTable<T> tab;
+};
+
+template <typename T>
+__device__ __forceinline__ void cb_ray(const CBParams<T> &p, int ia, int ib, int iv, T *r)
+{
+    cb_ray(p.rg, p.tab.cs[iv], p.tab.sn[iv], p.tab.off[iv], ia, ib, r);
+}
+
+// Detector cell of this thread (thread walk): 32 columns x blockDim.y rows
+// per CTA; grid (column tile, view, row band) when band_major, else (column
+// tile, row band, view).
+template <typename T>
+__device__ __forceinline__ void cb_cell(const CBParams<T> &p, int &ia, int &ib, int &iv)
+{
+    ia = blockIdx.x * 32 + threadIdx.x;
+    if (p.band_major) { iv = blockIdx.y; ib = blockIdx.z * blockDim.y + threadIdx.y; }
+    else { ib = blockIdx.y * blockDim.y + threadIdx.y; iv = blockIdx.z; }
+}
+
+// Sinogram value of a ray for the transpose; Q8: the reference's cylindrical
+// backprojection reads ia + iv*na + ib*na*nb (reads past the end count as 0).
+template <typename T> __device__ __forceinline__ T cb_sino_value(const CBParams<T> &p, int ia, int ib, int iv)
+{
+    const size_t total = (size_t)p.na * p.nb * p.nv_total;
+    const size_t vg = (size_t)(p.v0 + iv);
+    const size_t id = (p.flags & NEFCT_Q8_INDEX) ? (size_t)ia + vg * p.na + (size_t)ib * p.na * p.nb
+                                                 : vg * p.na * p.nb + (size_t)ib * p.na + ia;
+    return id < total ? p.sino[id] : (T)0;
+}
+
+template <typename T, bool DIV, bool EXACT = false>
+__global__ void __launch_bounds__(256) cb_forward_kernel(const __grid_constant__ CBParams<T> p)
+{
+    int ia, ib, iv;
+    cb_cell(p, ia, ib, iv);
+    if (ia >= p.na || ib >= p.nb) return;
+    T r[6];
+    cb_ray(p, ia, ib, iv, r);
+    const T acc = ray_forward<T, DIV, EXACT>(p.g, r, p.flags, p.vol, p.volT);
+    p.out[(size_t)(p.v0 + iv) * p.na * p.nb + (size_t)ib * p.na + ia] = acc;
+}
+
+template <typename T, bool DIV, bool EXACT = false>
+__global__ void __launch_bounds__(256) cb_backward_kernel(const __grid_constant__ CBParams<T> p)
+{
+    int ia, ib, iv;
+    cb_cell(p, ia, ib, iv);
+    if (ia >= p.na || ib >= p.nb) return;
+    const T y = cb_sino_value(p, ia, ib, iv);
+    if (y == (T)0) return;
+    T r[6];
+    cb_ray(p, ia, ib, iv, r);
+    ray_backward<T, DIV, EXACT>(p.g, r, p.flags, y, p.out, p.outT);
+}
+
+// Column warps: warp = rows [32*tile, 32*tile + 32) of column ia at view iv.
+// FWD: gathers from the z-fastest copy p.volT into the sinogram p.out;
+// otherwise reduces into the z-fastest accumulator p.outT.  Rays without a
+// contribution (outside the detector, missing the grid, zero value) stay in
+// the warp's walk with every slot inactive.
+template <bool DIV, bool FWD>
+__global__ void __launch_bounds__(256) cb_colwarp_kernel(const __grid_constant__ CBParams<float> p)
+{
+    const int lane = threadIdx.x;
+    const int ia = blockIdx.x * blockDim.y + threadIdx.y;
+    int ib, iv;
+    if (p.band_major) { iv = blockIdx.y; ib = blockIdx.z * 32 + lane; }
+    else { ib = blockIdx.y * 32 + lane; iv = blockIdx.z; }
+    if (ia >= p.na) return;                       // uniform across the warp
+    const bool has = ib < p.nb;
+    float y = 0.f;
+    if (!FWD && has) y = cb_sino_value(p, ia, ib, iv);
+    float r[6];
+    cb_ray(p, ia, has ? ib : 0, iv, r);
+    Walk<float> w{};
+    const bool live = has && (FWD || y != 0.f) && setup_walk(p.g, r, p.flags, w);
+    float *const sino_out = FWD ? p.out + (size_t)(p.v0 + iv) * p.na * p.nb + (size_t)ib * p.na + ia : nullptr;
+    if (!__any_sync(0xffffffffu, live)) {
+        if (FWD && has) *sino_out = 0.f;
+        return;
+    }
+    ColShared c;
+    ColLane L;
+    int K0, K1, KI0, KI1;
+    if (!col_setup(p.g, w, live, c, L, K0, K1, KI0, KI1)) {
+        // rays of the column disagree on the shared parameters: walk alone
+        unsigned su, sv;
+        col_strides(p.g, w.xdrive, su, sv);
+        if (FWD) {
+            const float v = live ? gather_walk<float, DIV, false, false>(w, p.g, p.volT, (int)su, (int)sv, 1) : 0.f;
+            if (has) *sino_out = v;
+        } else if (live) {
+            scatter_walk<float, DIV, false, false>(w, p.g, p.outT, (int)su, (int)sv, 1, y);
+        }
+        return;
+    }
+    if (FWD) {
+        const float *__restrict__ src = p.volT;
+        float acc = 0.f;
+        auto f = [&](const SlabSlots<float> &s) {
+            const float v0 = s.ok[0] ? __ldg(src + s.idx[0]) : 0.f;
+            const float v1 = s.ok[1] ? __ldg(src + s.idx[1]) : 0.f;
+            const float v2 = s.ok[2] ? __ldg(src + s.idx[2]) : 0.f;
+            acc += v0 * s.r[0];
+            acc += v1 * s.r[1];
+            acc += v2 * s.r[2];
+        };
+        col_walk_any<DIV>(c, L, K0, K1, KI0, KI1, p.g, f);
+        if (has) *sino_out = live ? acc * w.W : 0.f;
+    } else {
+        float *dst = p.outT;
+        const float yw = y * w.W;
+        auto f = [&](const SlabSlots<float> &s) {
+            if (s.ok[0]) atomicAdd(dst + s.idx[0], yw * s.r[0]);
+            if (s.ok[1]) atomicAdd(dst + s.idx[1], yw * s.r[1]);
+            if (s.ok[2]) atomicAdd(dst + s.idx[2], yw * s.r[2]);
+        };
+        col_walk_any<DIV>(c, L, K0, K1, KI0, KI1, p.g, f);
+    }
+}
+
+// Launch shape of the thread walk for nvc views (see cb_cell).
+template <typename T>
+static inline void cb_shape(CBParams<T> &p, int na, int nb, int nvc, dim3 &grid, dim3 &block)
+{
+    const int rows = tune_get(NEFCT_TUNE_CB_ROWS);
+    p.band_major = tune_get(NEFCT_TUNE_CB_ORDER) == 0;
+    block = dim3(32, rows);
+    const unsigned bands = (unsigned)((nb + rows - 1) / rows);
+    grid = p.band_major ? dim3((na + 31) / 32, nvc, bands) : dim3((na + 31) / 32, bands, nvc);
+}
+
+// Launch shape of the column warps: NEFCT_TUNE_CB_ROWS columns (warps) per
+// CTA, 32 rows per warp.
+template <typename T>
+static inline void cb_colwarp_shape(CBParams<T> &p, int na, int nb, int nvc, dim3 &grid, dim3 &block)
+{
+    const int cols = tune_get(NEFCT_TUNE_CB_ROWS);
+    p.band_major = tune_get(NEFCT_TUNE_CB_ORDER) == 0;
+    block = dim3(32, cols);
+    const unsigned tiles = (unsigned)((nb + 31) / 32);
+    grid = p.band_major ? dim3((na + cols - 1) / cols, nvc, tiles) : dim3((na + cols - 1) / cols, tiles, nvc);
+}
+
+// The walk skips its divisions when both transverse pitches equal the x pitch.
+template <typename T> static inline bool cubic(const GridDev<T> &g) { return g.dy == (T)1 && g.dz == (T)1; }
+
+// Column warps apply to FP32 slab walks with a workspace; the z-fastest
+// copy's transposes launch ny planes (grid z), and the packed v floors hold
+// n + 3 in 16 bits.
+template <typename T> static inline bool cb_use_colwarp(const nefct_grid &g, uint32_t flags, bool forward)
+{
+    return sizeof(T) == sizeof(float) && (tune_get(NEFCT_TUNE_CB_WALK) & (forward ? 1 : 2)) != 0 &&
+           !(flags & (NEFCT_EXACT | NEFCT_NO_TRANSPOSE | NEFCT_DETERMINISTIC)) && g.ny <= 65535 &&
+           g.nx + 3 < 65536 && g.ny + 3 < 65536;
+}
+
+// Launches the thread-walk forward (FWD) or transpose kernel for the views
+// set in p.
+template <typename T, bool FWD>
+static inline cudaError_t cb_launch(CBParams<T> &p, int na, int nb, int nvc, uint32_t flags, cudaStream_t s)
+{
+    dim3 grid, block;
+    cb_shape(p, na, nb, nvc, grid, block);
+    const bool exact = (flags & NEFCT_EXACT) != 0, div = !cubic(p.g);
+    if constexpr (FWD) {
+        if (exact) cb_forward_kernel<T, false, true><<<grid, block, 0, s>>>(p);
+        else if (div) cb_forward_kernel<T, true><<<grid, block, 0, s>>>(p);
+        else cb_forward_kernel<T, false><<<grid, block, 0, s>>>(p);
+    } else {
+        if (exact) cb_backward_kernel<T, false, true><<<grid, block, 0, s>>>(p);
+        else if (div) cb_backward_kernel<T, true><<<grid, block, 0, s>>>(p);
+        else cb_backward_kernel<T, false><<<grid, block, 0, s>>>(p);
+    }
+    return cudaGetLastError();
+}
+
+template <bool FWD>
+static inline cudaError_t cb_launch_colwarp(CBParams<float> &p, int na, int nb, int nvc, cudaStream_t s)
+{
+    dim3 grid, block;
+    cb_colwarp_shape(p, na, nb, nvc, grid, block);
+    if (cubic(p.g)) cb_colwarp_kernel<false, FWD><<<grid, block, 0, s>>>(p);
+    else cb_colwarp_kernel<true, FWD><<<grid, block, 0, s>>>(p);
+    return cudaGetLastError();
+}
+
+// Launches the forward / transpose kernels for the views set in p: the
+// thread walk, or the column warps when colwarp (p.volT / p.outT then hold
+// the z-fastest copy / accumulator).  Defined in cb_forward.cu /
+// cb_backward.cu for float and double.
+template <typename T>
+cudaError_t cb_launch_forward(CBParams<T> &p, int na, int nb, int nvc, uint32_t flags, cudaStream_t s,
+                              bool colwarp = false);
+template <typename T>
+cudaError_t cb_launch_backward(CBParams<T> &p, int na, int nb, int nvc, uint32_t flags, cudaStream_t s,
+                               bool colwarp = false);
+
+}  // namespace nefct

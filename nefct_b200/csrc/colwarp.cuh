@@ -1,0 +1,223 @@
+// Column-warp cone-beam walk (FP32, sm_100a).
+//
+// The rays of one detector column at one view share their x and y end
+// points (the generator's x1, y1, x2, y2 do not depend on the row: the
+// source and the column's detector points lie in one vertical plane), so the
+// drive axis, pu, pv, kv and every transverse (v) plane position, floor and
+// crossing ratio are bit-identical across the rows of a column; only the z
+// part (pw, kw, W) differs.
+//
+// One warp walks 32 consecutive rows of one column in lockstep over the
+// union of their slab ranges:
+//  * the v part of each slab is computed once per warp: lane j builds the
+//    entry of slab kc + j of a 32-slab chunk, and each slab's entry is
+//    broadcast with shuffles (3 per interior slab, 4 per boundary slab);
+//  * each lane evaluates the z part and the three-voxel split of its own
+//    ray exactly as the single-ray walker does (same operations, same order);
+//  * the volume (forward) and the accumulator (transpose) are z-fastest
+//    copies [y][x][z]: the 32 rows of a warp sit at neighbouring z of the
+//    same (u, v) voxel column, so a warp's gather or reduction touches one or
+//    two 32-byte sectors instead of one per row band.
+// Slabs outside a ray's own range lie outside the grid for that ray and the
+// boundary checks reject them; the warp's check-free (interior) range is the
+// intersection of its rays' interior ranges.
+#pragma once
+
+#include <limits.h>
+
+#include "siddon.cuh"
+
+namespace nefct {
+
+// v part of one slab: biased bases of the low/high v voxel columns (index of
+// (k, v, z) = b + floor bits of z), the clamped v floors for the boundary
+// checks, and the v crossing ratio.
+struct ColEntry {
+    unsigned b1, b2;    // k*su + c*sv - 0x4B400000 for the low/high v floor c
+    unsigned cv;        // (c1 + 2) | (c2 + 2) << 16, c clamped to [-2, nv + 1]
+    float rv;           // crossing ratio, 1 without a v crossing
+};
+
+// Shared (warp-uniform) parameters of the column's walk.
+struct ColShared {
+    float pu, pv, kv, dv, nv2, nu2;
+    int nv;
+    unsigned su, sv;
+    bool vdiv;
+};
+
+// Entry of slab k: planes t = k - nu2 and t + 1, positions and floors as in
+// Walker::pos / Walker::next (same operations and order), so every value
+// equals the single-ray walker's.  Clamping a floor to [-2, nv + 1] keeps
+// every admission decision of the boundary checks.
+template <bool DIV> __device__ __forceinline__ ColEntry col_entry(const ColShared &c, int k)
+{
+    const float ta = __fsub_rn((float)k, c.nu2), tb = __fadd_rn(ta, 1.f);
+    auto vpos = [&](float t) {
+        float q = __fadd_rn(c.pv, __fmul_rn(c.kv, __fsub_rn(t, c.pu)));
+        if (DIV && c.vdiv) q = __fdiv_rn(q, c.dv);
+        return __fadd_rn(q, c.nv2);
+    };
+    const float qa = vpos(ta), qb = vpos(tb);
+    const float ma = magic_floor<true>(qa), mb = magic_floor<true>(qb);
+    const float q1 = fminf(qa, qb), q2 = fmaxf(qa, qb);
+    const float m1 = fminf(ma, mb), m2 = fmaxf(ma, mb);
+    ColEntry e;
+    e.rv = m1 != m2 ? FP<float>::ratio(__fadd_rn(__fadd_rn(m2, -kFloorMagic), -q1), __fadd_rn(q2, -q1)) : 1.f;
+    const int c1 = min(max(__float_as_int(m1) - kFloorMagicBits, -2), c.nv + 1);
+    const int c2 = min(max(__float_as_int(m2) - kFloorMagicBits, -2), c.nv + 1);
+    const unsigned base = (unsigned)k * c.su - (unsigned)kFloorMagicBits;
+    e.b1 = base + (unsigned)c1 * c.sv;
+    e.b2 = base + (unsigned)c2 * c.sv;
+    e.cv = (unsigned)(c1 + 2) | ((unsigned)(c2 + 2) << 16);
+    return e;
+}
+
+// Per-lane z state of the walk.
+struct ColLane {
+    float pw, kw, qaw, maw;
+    bool live, up;
+};
+
+// One slab of the lane's ray.  WUP: 1 every live ray has kw >= 0, 0 every
+// live ray has kw < 0, 2 mixed (per-lane choice).
+template <bool DIV, bool CHECK, int WUP>
+__device__ __forceinline__ SlabSlots<float> col_slab(ColLane &L, float d, float dz, bool zdiv, float nz2, int nv,
+                                                     int nz, const ColEntry &e, int j)
+{
+    const unsigned b1 = __shfl_sync(0xffffffffu, e.b1, j);
+    const unsigned b2 = __shfl_sync(0xffffffffu, e.b2, j);
+    const float rv = __shfl_sync(0xffffffffu, e.rv, j);
+    unsigned cv = 0;
+    if (CHECK) cv = __shfl_sync(0xffffffffu, e.cv, j);
+
+    float qbw = __fadd_rn(L.pw, __fmul_rn(L.kw, d));
+    if (DIV && zdiv) qbw = __fdiv_rn(qbw, dz);
+    qbw = __fadd_rn(qbw, nz2);
+    const float mbw = magic_floor<CHECK>(qbw);
+    const bool up = WUP == 2 ? L.up : WUP == 1;
+    const float q1w = up ? L.qaw : qbw, q2w = up ? qbw : L.qaw;
+    const float m1w = up ? L.maw : mbw, m2w = up ? mbw : L.maw;
+    L.qaw = qbw;
+    L.maw = mbw;
+    const bool vx = b1 != b2, wx = m1w != m2w;
+    const float rw = wx ? FP<float>::ratio(__fadd_rn(__fadd_rn(m2w, -kFloorMagic), -q1w), __fadd_rn(q2w, -q1w)) : 1.f;
+    const bool vfirst = rv > rw;
+    const unsigned i1 = (unsigned)__float_as_int(m1w), i2 = (unsigned)__float_as_int(m2w);
+    SlabSlots<float> s;
+    s.r[0] = fminf(rv, rw);
+    s.r[1] = fabsf(__fsub_rn(rv, rw));
+    s.r[2] = __fsub_rn(1.f, fmaxf(rv, rw));
+    s.idx[0] = b1 + i1;
+    s.idx[1] = vfirst ? b1 + i2 : b2 + i1;
+    s.idx[2] = b2 + i2;
+    s.mid3 = vx && wx;
+    if (CHECK) {
+        // slab admission (reference siddon.cu.cc :80, :92, :112, :116, :132)
+        const int cv1 = (int)(cv & 0xffffu) - 2, cv2 = (int)(cv >> 16) - 2;
+        const int cw1 = (int)i1 - kFloorMagicBits, cw2 = (int)i2 - kFloorMagicBits;
+        const bool adm = L.live && (unsigned)(cv1 + (int)vx) < (unsigned)(nv + (int)vx) &&
+                         (unsigned)(cw1 + (int)wx) < (unsigned)(nz + (int)wx);
+        const int mv = vfirst ? cv1 : cv2, mw = vfirst ? cw2 : cw1;
+        s.ok[0] = adm && (cv1 | cw1) >= 0;
+        s.ok[1] = adm && (vx || wx) && (unsigned)mv < (unsigned)nv && (unsigned)mw < (unsigned)nz;
+        s.ok[2] = adm && vx && wx && cv2 < nv && cw2 < nz;
+    } else {
+        s.ok[0] = L.live;
+        s.ok[1] = L.live && (vx || wx);
+        s.ok[2] = L.live && vx && wx;
+    }
+    return s;
+}
+
+// Walks slabs [a, b] (inside the current 32-slab chunk starting at kc) in
+// one check mode.  t is the entry plane k - nu2 of slab k, carried exactly.
+template <bool DIV, bool CHECK, int WUP, class Fn>
+__device__ __forceinline__ void col_range(int a, int b, int kc, float &t, const ColShared &c, ColLane &L,
+                                          const ColEntry &e, const GridDev<float> &g, Fn &f)
+{
+    const bool zdiv = g.dz != 1.f;
+#pragma unroll 2
+    for (int k = a; k <= b; ++k) {
+        const float t2 = __fadd_rn(t, 1.f);
+        t = t2;
+        f(col_slab<DIV, CHECK, WUP>(L, __fsub_rn(t2, c.pu), g.dz, zdiv, g.nz2, c.nv, g.nz, e, k - kc));
+    }
+}
+
+// Slabs [K0, K1] of the warp in 32-slab chunks (lane j builds the entry of
+// slab kc + j); boundary slabs outside [KI0, KI1] with range checks.
+template <bool DIV, int WUP, class Fn>
+__device__ __forceinline__ void col_walk(const ColShared &c, ColLane &L, int K0, int K1, int KI0, int KI1,
+                                         const GridDev<float> &g, Fn &f)
+{
+    // plane K0 - nu2 (entry plane of the first slab)
+    float t = __fsub_rn((float)K0, c.nu2);
+    float q = __fadd_rn(L.pw, __fmul_rn(L.kw, __fsub_rn(t, c.pu)));
+    if (DIV && g.dz != 1.f) q = __fdiv_rn(q, g.dz);
+    L.qaw = __fadd_rn(q, g.nz2);
+    L.maw = magic_floor<true>(L.qaw);
+    const int lane = threadIdx.x & 31;
+    if (KI0 > KI1) { KI0 = K1 + 1; KI1 = K1; }      // no interior: everything checked
+    for (int kc = K0; kc <= K1; kc += 32) {
+        const ColEntry e = col_entry<DIV>(c, kc + lane);
+        const int ke = min(K1, kc + 31);
+        col_range<DIV, true, WUP>(kc, min(ke, KI0 - 1), kc, t, c, L, e, g, f);
+        col_range<DIV, false, WUP>(max(kc, KI0), min(ke, KI1), kc, t, c, L, e, g, f);
+        col_range<DIV, true, WUP>(max(kc, KI1 + 1), ke, kc, t, c, L, e, g, f);
+    }
+}
+
+template <bool DIV, class Fn>
+__device__ __forceinline__ void col_walk_any(const ColShared &c, ColLane &L, int K0, int K1, int KI0, int KI1,
+                                             const GridDev<float> &g, Fn &f)
+{
+    const bool all_up = __all_sync(0xffffffffu, L.up || !L.live);
+    const bool all_down = __all_sync(0xffffffffu, !L.up || !L.live);
+    if (all_up) col_walk<DIV, 1>(c, L, K0, K1, KI0, KI1, g, f);
+    else if (all_down) col_walk<DIV, 0>(c, L, K0, K1, KI0, KI1, g, f);
+    else col_walk<DIV, 2>(c, L, K0, K1, KI0, KI1, g, f);
+}
+
+// Strides of the z-fastest layout [y][x][z] along (u, v) of the drive axis.
+__device__ __forceinline__ void col_strides(const GridDev<float> &g, bool xdrive, unsigned &su, unsigned &sv)
+{
+    const unsigned xs = (unsigned)g.nz, ys = (unsigned)g.nx * (unsigned)g.nz;
+    su = xdrive ? xs : ys;
+    sv = xdrive ? ys : xs;
+}
+
+// Sets up the warp: shared parameters from the first live lane, the warp's
+// slab and interior ranges.  Returns false when the rays do not share their
+// v parameters bit for bit (each lane then walks alone).
+__device__ __forceinline__ bool col_setup(const GridDev<float> &g, const Walk<float> &w, bool live, ColShared &c,
+                                          ColLane &L, int &K0, int &K1, int &KI0, int &KI1)
+{
+    const unsigned lm = __ballot_sync(0xffffffffu, live);
+    const int src = __ffs(lm) - 1;
+    c.pu = __shfl_sync(0xffffffffu, w.pu, src);
+    c.pv = __shfl_sync(0xffffffffu, w.pv, src);
+    c.kv = __shfl_sync(0xffffffffu, w.kv, src);
+    const bool xdrive = __shfl_sync(0xffffffffu, (int)w.xdrive, src) != 0;
+    const bool same = !live || (__float_as_int(w.pu) == __float_as_int(c.pu) &&
+                                __float_as_int(w.pv) == __float_as_int(c.pv) &&
+                                __float_as_int(w.kv) == __float_as_int(c.kv) && w.xdrive == xdrive);
+    if (!__all_sync(0xffffffffu, same)) return false;
+    c.dv = xdrive ? g.dy : 1.f;
+    c.vdiv = xdrive && g.dy != 1.f;
+    c.nv2 = xdrive ? g.ny2 : g.nx2;
+    c.nu2 = xdrive ? g.nx2 : g.ny2;
+    c.nv = xdrive ? g.ny : g.nx;
+    col_strides(g, xdrive, c.su, c.sv);
+    K0 = __reduce_min_sync(0xffffffffu, live ? w.k0 : INT_MAX);
+    K1 = __reduce_max_sync(0xffffffffu, live ? w.k1 : INT_MIN);
+    KI0 = __reduce_max_sync(0xffffffffu, live ? w.ki0 : INT_MIN);
+    KI1 = __reduce_min_sync(0xffffffffu, live ? w.ki1 : INT_MAX);
+    L.pw = w.pw;
+    L.kw = w.kw;
+    L.live = live;
+    L.up = w.kw >= 0.f;
+    return true;
+}
+
+}  // namespace nefct

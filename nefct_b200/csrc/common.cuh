@@ -29,6 +29,14 @@ nefct_status cuda_fail(cudaError_t e, const char *what);
         if (e_ != cudaSuccess) return ::nefct::cuda_fail(e_, name); \
     } while (0)
 
+// Approximate reciprocal (PTX rcp.approx.ftz.f32, relative error <= 2^-23).
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // Arithmetic with explicit round-to-nearest so the compiler cannot contract
 // a*b+c into one fused operation where the reference's evaluation order has
 // two roundings.  Used for every quantity that feeds a floor() or a branch.
@@ -40,8 +48,8 @@ template <> struct FP<float> {
     static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
     static __device__ __forceinline__ float sqrt(float a) { return __fsqrt_rn(a); }
     static __device__ __forceinline__ int ifloor(float a) { return __float2int_rd(a); }
-    // ratio of a crossing: fast division, error <= 2 ulp
-    static __device__ __forceinline__ float ratio(float a, float b) { return __fdividef(a, b); }
+    // ratio of a crossing: a times the approximate reciprocal of b (<= 2 ulp)
+    static __device__ __forceinline__ float ratio(float a, float b) { return __fmul_rn(a, rcp_approx(b)); }
     static __device__ __forceinline__ float min(float a, float b) { return fminf(a, b); }
     static __device__ __forceinline__ float max(float a, float b) { return fmaxf(a, b); }
     static __device__ __forceinline__ float abs(float a) { return fabsf(a); }

@@ -1,89 +1,22 @@
-// Cone-beam and LOR Siddon projectors on sm_100a, and their C-ABI entry
-// points (declared in include/nefct_b200.h).
+// Cone-beam and LOR Siddon projectors on sm_100a: host side of the cone-beam
+// projector (validation, per-view tables, workspace, transposes, the
+// deterministic transpose), the intersection count, the LOR pair and the
+// C-ABI entry points (declared in include/nefct_b200.h).  The cone-beam
+// kernels themselves are in cb_kernels.cuh.
 //
-// Launch shape: one thread per ray; a 256-thread CTA covers 32 adjacent
-// detector columns x 8 rows of one view, so each warp is 32 neighbouring
-// columns of one row.  The grid runs (column tile, view, row band) with the
-// row band slowest: the CTAs in flight cover all views of one band of rows,
-// whose rays only reach a thin z-slab of the volume, so the gathered volume
-// (forward) or the reduced accumulator (transpose) stays resident in L2
-// instead of every view sweeping the whole volume through it.  Neighbouring rays of a warp cross a driving slab at
-// neighbouring transverse positions; with the transverse axis contiguous in
-// memory a warp's gather touches one or two 128-byte lines.  That holds for
-// y-driven rays in the x-fastest volume; x-driven rays read a y-fastest copy
-// of the volume (one transpose per call, in the caller's workspace).
-// Per-view cos/sin/z-offset ride in the kernel parameters.
+// Neighbouring rays of a warp cross a driving slab at neighbouring
+// transverse positions; with the transverse axis contiguous in memory a
+// warp's gather touches one or two 128-byte lines.  That holds for y-driven
+// rays in the x-fastest volume; x-driven rays read a y-fastest copy of the
+// volume (one transpose per call, in the caller's workspace).
 #include <math.h>
 #include <algorithm>
 #include <mutex>
+#include <type_traits>
 
-#include "siddon.cuh"
+#include "cb_kernels.cuh"
 
 namespace nefct {
-
-template <typename T> struct CBParams {
-    GridDev<T> g;
-    int na, nb, nvc, v0, nv_total;
-    RayGeom<T> rg;
-    int band_major;
-    uint32_t flags;
-    const T *vol;        // x-fastest volume (forward source)
-    const T *volT;       // y-fastest copy for x-driven rays, or nullptr
-    const T *sino;       // backward source, full sinogram
-    T *out;              // forward: full sinogram; backward: x-fastest volume
-    T *outT;             // backward: y-fastest accumulator, or nullptr
-    unsigned long long *fix, *fixT;   // deterministic backward: integer accumulators
-    const float *fix_scale;           // deterministic backward: power-of-two scale (device)
-    unsigned long long *count;
-    ViewTable<T> tab;
-};
-
-template <typename T>
-__device__ __forceinline__ void cb_ray(const CBParams<T> &p, int ia, int ib, int iv, T *r)
-{
-    cb_ray(p.rg, p.tab.cs[iv], p.tab.sn[iv], p.tab.off[iv], ia, ib, r);
-}
-
-// Detector cell of this thread: 32 columns x blockDim.y rows per CTA; grid
-// (column tile, view, row band) when band_major, else (column tile, row
-// band, view).
-template <typename T>
-__device__ __forceinline__ void cb_cell(const CBParams<T> &p, int &ia, int &ib, int &iv)
-{
-    ia = blockIdx.x * 32 + threadIdx.x;
-    if (p.band_major) { iv = blockIdx.y; ib = blockIdx.z * blockDim.y + threadIdx.y; }
-    else { ib = blockIdx.y * blockDim.y + threadIdx.y; iv = blockIdx.z; }
-}
-
-template <typename T, bool DIV, bool EXACT = false>
-__global__ void __launch_bounds__(256) cb_forward_kernel(const __grid_constant__ CBParams<T> p)
-{
-    int ia, ib, iv;
-    cb_cell(p, ia, ib, iv);
-    if (ia >= p.na || ib >= p.nb) return;
-    T r[6];
-    cb_ray(p, ia, ib, iv, r);
-    const T acc = ray_forward<T, DIV, EXACT>(p.g, r, p.flags, p.vol, p.volT);
-    p.out[(size_t)(p.v0 + iv) * p.na * p.nb + (size_t)ib * p.na + ia] = acc;
-}
-
-template <typename T, bool DIV, bool EXACT = false>
-__global__ void __launch_bounds__(256) cb_backward_kernel(const __grid_constant__ CBParams<T> p)
-{
-    int ia, ib, iv;
-    cb_cell(p, ia, ib, iv);
-    if (ia >= p.na || ib >= p.nb) return;
-    const size_t total = (size_t)p.na * p.nb * p.nv_total;
-    const size_t vg = (size_t)(p.v0 + iv);
-    // Q8: the reference's cylindrical backprojection reads ia + iv*na + ib*na*nb
-    const size_t id = (p.flags & NEFCT_Q8_INDEX) ? (size_t)ia + vg * p.na + (size_t)ib * p.na * p.nb
-                                                 : vg * p.na * p.nb + (size_t)ib * p.na + ia;
-    const T y = id < total ? p.sino[id] : (T)0;
-    if (y == (T)0) return;
-    T r[6];
-    cb_ray(p, ia, ib, iv, r);
-    ray_backward<T, DIV, EXACT>(p.g, r, p.flags, y, p.out, p.outT);
-}
 
 template <bool DIV>
 __global__ void __launch_bounds__(256) cb_count_kernel(const __grid_constant__ CBParams<float> p)
@@ -109,11 +42,7 @@ __global__ void __launch_bounds__(256) cb_backward_fixed_kernel(const __grid_con
     int ia, ib, iv;
     cb_cell(p, ia, ib, iv);
     if (ia >= p.na || ib >= p.nb) return;
-    const size_t total = (size_t)p.na * p.nb * p.nv_total;
-    const size_t vg = (size_t)(p.v0 + iv);
-    const size_t id = (p.flags & NEFCT_Q8_INDEX) ? (size_t)ia + vg * p.na + (size_t)ib * p.na * p.nb
-                                                 : vg * p.na * p.nb + (size_t)ib * p.na + ia;
-    const float y = id < total ? p.sino[id] : 0.f;
+    const float y = cb_sino_value(p, ia, ib, iv);
     if (y == 0.f) return;
     float r[6];
     cb_ray(p, ia, ib, iv, r);
@@ -223,19 +152,6 @@ __global__ void __launch_bounds__(256) lor_backward_kernel(const __grid_constant
 
 // ---------------- host side ----------------
 
-// Launch shape of the cone-beam kernels for nvc views (see cb_cell).
-template <typename T> static void cb_shape(CBParams<T> &p, int na, int nb, int nvc, dim3 &grid, dim3 &block)
-{
-    const int rows = tune_get(NEFCT_TUNE_CB_ROWS);
-    p.band_major = tune_get(NEFCT_TUNE_CB_ORDER) == 0;
-    block = dim3(32, rows);
-    const unsigned bands = (unsigned)((nb + rows - 1) / rows);
-    grid = p.band_major ? dim3((na + 31) / 32, nvc, bands) : dim3((na + 31) / 32, bands, nvc);
-}
-
-// The walk skips its divisions when both transverse pitches equal the x pitch.
-template <typename T> static bool cubic(const GridDev<T> &g) { return g.dy == (T)1 && g.dz == (T)1; }
-
 static const uint32_t kWalkFlags = NEFCT_TIE_GT | NEFCT_SKIP_SHORT | NEFCT_NO_INV_L2 | NEFCT_Q5 |
                                    NEFCT_Q8_INDEX | NEFCT_NO_TRANSPOSE | NEFCT_DETERMINISTIC | NEFCT_EXACT;
 
@@ -243,6 +159,8 @@ static nefct_status check_grid(const nefct_grid &g)
 {
     if (g.nx < 1 || g.ny < 1 || g.nz < 1)
         return fail(NEFCT_ERR_INVALID, "grid dimensions must be >= 1 (got %d x %d x %d)", g.nx, g.ny, g.nz);
+    if (g.nx > (1 << 20) || g.ny > (1 << 20) || g.nz > (1 << 20))
+        return fail(NEFCT_ERR_INVALID, "grid dimensions must be <= 2^20 (got %d x %d x %d)", g.nx, g.ny, g.nz);
     if ((long long)g.nx * g.ny * g.nz >= (1ll << 31))
         return fail(NEFCT_ERR_INVALID, "grid has %lld voxels; at most 2^31-1 are supported",
                     (long long)g.nx * g.ny * g.nz);
@@ -299,6 +217,58 @@ template <typename T> static void fill_views(CBParams<T> &p, const nefct_cb_geom
     }
 }
 
+// volZ[y][x][z] = vol[z][y][x]  (32x32 tiles of each y plane)
+__global__ void __launch_bounds__(256) zmajor_kernel(const float *__restrict__ in, float *__restrict__ out, int nx,
+                                                     int ny, int nz)
+{
+    __shared__ float tile[32][33];
+    const int y = blockIdx.z, x0 = blockIdx.x * 32, z0 = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int x = x0 + threadIdx.x, z = z0 + j;
+        if (x < nx && z < nz) tile[j][threadIdx.x] = in[((size_t)z * ny + y) * nx + x];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int x = x0 + j, z = z0 + threadIdx.x;
+        if (x < nx && z < nz) out[((size_t)y * nx + x) * nz + z] = tile[threadIdx.x][j];
+    }
+}
+
+// vol[z][y][x] = accZ[y][x][z]
+__global__ void __launch_bounds__(256) zfold_kernel(const float *__restrict__ acc, float *__restrict__ vol, int nx,
+                                                    int ny, int nz)
+{
+    __shared__ float tile[32][33];
+    const int y = blockIdx.z, x0 = blockIdx.x * 32, z0 = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int x = x0 + j, z = z0 + threadIdx.x;
+        if (x < nx && z < nz) tile[j][threadIdx.x] = acc[((size_t)y * nx + x) * nz + z];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int x = x0 + threadIdx.x, z = z0 + j;
+        if (x < nx && z < nz) vol[((size_t)z * ny + y) * nx + x] = tile[threadIdx.x][j];
+    }
+}
+
+// z-fastest copy [y][x][z] of an x-fastest volume (column-warp forward)
+static nefct_status zmajor_copy(const float *in, float *out, const nefct_grid &g, cudaStream_t s)
+{
+    dim3 grid((g.nx + 31) / 32, (g.nz + 31) / 32, g.ny);
+    zmajor_kernel<<<grid, dim3(32, 8), 0, s>>>(in, out, g.nx, g.ny, g.nz);
+    NEFCT_CHECK_LAUNCH("zmajor_kernel");
+    return NEFCT_OK;
+}
+
+// vol = the x-fastest layout of the z-fastest accumulator (column-warp transpose)
+static nefct_status zfold(const float *acc, float *vol, const nefct_grid &g, cudaStream_t s)
+{
+    dim3 grid((g.nx + 31) / 32, (g.nz + 31) / 32, g.ny);
+    zfold_kernel<<<grid, dim3(32, 8), 0, s>>>(acc, vol, g.nx, g.ny, g.nz);
+    NEFCT_CHECK_LAUNCH("zfold_kernel");
+    return NEFCT_OK;
+}
+
 template <typename T>
 static nefct_status transpose_xy(const T *in, T *out, const nefct_grid &g, cudaStream_t s)
 {
@@ -322,12 +292,8 @@ nefct_status cb_forward_launches(const nefct_cb_geom *g, const float *vol, const
     for (int v0 = 0; v0 < g->nv; v0 += ViewTable<float>::kMax) {
         const int nvc = std::min(ViewTable<float>::kMax, g->nv - v0);
         fill_views(p, g, v0, nvc);
-        dim3 grid, block;
-        cb_shape(p, g->na, g->nb, nvc, grid, block);
-        if (flags & NEFCT_EXACT) cb_forward_kernel<float, false, true><<<grid, block, 0, s>>>(p);
-        else if (cubic(p.g)) cb_forward_kernel<float, false><<<grid, block, 0, s>>>(p);
-        else cb_forward_kernel<float, true><<<grid, block, 0, s>>>(p);
-        NEFCT_CHECK_LAUNCH("cb_forward_kernel");
+        const cudaError_t e = cb_launch_forward<float>(p, g->na, g->nb, nvc, flags, s);
+        if (e != cudaSuccess) return cuda_fail(e, "cb_forward_kernel");
     }
     return NEFCT_OK;
 }
@@ -343,12 +309,8 @@ nefct_status cb_backward_launches(const nefct_cb_geom *g, const float *sino, flo
     for (int v0 = 0; v0 < g->nv; v0 += ViewTable<float>::kMax) {
         const int nvc = std::min(ViewTable<float>::kMax, g->nv - v0);
         fill_views(p, g, v0, nvc);
-        dim3 grid, block;
-        cb_shape(p, g->na, g->nb, nvc, grid, block);
-        if (flags & NEFCT_EXACT) cb_backward_kernel<float, false, true><<<grid, block, 0, s>>>(p);
-        else if (cubic(p.g)) cb_backward_kernel<float, false><<<grid, block, 0, s>>>(p);
-        else cb_backward_kernel<float, true><<<grid, block, 0, s>>>(p);
-        NEFCT_CHECK_LAUNCH("cb_backward_kernel");
+        const cudaError_t e = cb_launch_backward<float>(p, g->na, g->nb, nvc, flags, s);
+        if (e != cudaSuccess) return cuda_fail(e, "cb_backward_kernel");
     }
     return NEFCT_OK;
 }
@@ -366,12 +328,18 @@ static nefct_status cb_forward_impl(const nefct_cb_geom *g, const T *vol, T *sin
     p->vol = vol;
     p->out = sino;
     const size_t nvox = (size_t)g->grid.nx * g->grid.ny * g->grid.nz;
+    const bool cw = cb_use_colwarp<T>(g->grid, flags, true);
     if (!(flags & NEFCT_NO_TRANSPOSE)) {
         if (!ws || wsb < nvox * sizeof(T)) {
             delete p;
             return fail(NEFCT_ERR_WORKSPACE, "forward needs %zu workspace bytes, got %zu", nvox * sizeof(T), wsb);
         }
-        st = transpose_xy(vol, (T *)ws, g->grid, s);
+        if constexpr (std::is_same<T, float>::value) {
+            if (cw) st = zmajor_copy(vol, (float *)ws, g->grid, s);
+            else st = transpose_xy(vol, (T *)ws, g->grid, s);
+        } else {
+            st = transpose_xy(vol, (T *)ws, g->grid, s);
+        }
         if (st) { delete p; return st; }
         p->volT = (const T *)ws;
     }
@@ -379,12 +347,7 @@ static nefct_status cb_forward_impl(const nefct_cb_geom *g, const T *vol, T *sin
     for (int v0 = 0; v0 < g->nv; v0 += kMax) {
         const int nvc = std::min(kMax, g->nv - v0);
         fill_views(*p, g, v0, nvc);
-        dim3 grid, block;
-        cb_shape(*p, g->na, g->nb, nvc, grid, block);
-        if (flags & NEFCT_EXACT) cb_forward_kernel<T, false, true><<<grid, block, 0, s>>>(*p);
-        else if (cubic(p->g)) cb_forward_kernel<T, false><<<grid, block, 0, s>>>(*p);
-        else cb_forward_kernel<T, true><<<grid, block, 0, s>>>(*p);
-        cudaError_t e = cudaGetLastError();
+        cudaError_t e = cb_launch_forward<T>(*p, g->na, g->nb, nvc, flags, s, cw);
         if (e != cudaSuccess) { delete p; return cuda_fail(e, "cb_forward_kernel"); }
     }
     delete p;
@@ -479,22 +442,23 @@ static nefct_status cb_backward_impl(const nefct_cb_geom *g, const T *sino, T *v
     p->sino = sino;
     p->out = vol;
     p->outT = tr ? (T *)ws : nullptr;
-    cudaError_t e = cudaMemsetAsync(vol, 0, nvox * sizeof(T), s);
+    // column warps reduce into the z-fastest workspace only; the fold then
+    // writes every voxel of vol
+    const bool cw = cb_use_colwarp<T>(g->grid, flags, false);
+    cudaError_t e = cw ? cudaSuccess : cudaMemsetAsync(vol, 0, nvox * sizeof(T), s);
     if (e == cudaSuccess && tr) e = cudaMemsetAsync(ws, 0, nvox * sizeof(T), s);
     if (e != cudaSuccess) { delete p; return cuda_fail(e, "cudaMemsetAsync"); }
     const int kMax = ViewTable<T>::kMax;
     for (int v0 = 0; v0 < g->nv; v0 += kMax) {
         const int nvc = std::min(kMax, g->nv - v0);
         fill_views(*p, g, v0, nvc);
-        dim3 grid, block;
-        cb_shape(*p, g->na, g->nb, nvc, grid, block);
-        if (flags & NEFCT_EXACT) cb_backward_kernel<T, false, true><<<grid, block, 0, s>>>(*p);
-        else if (cubic(p->g)) cb_backward_kernel<T, false><<<grid, block, 0, s>>>(*p);
-        else cb_backward_kernel<T, true><<<grid, block, 0, s>>>(*p);
-        e = cudaGetLastError();
+        e = cb_launch_backward<T>(*p, g->na, g->nb, nvc, flags, s, cw);
         if (e != cudaSuccess) { delete p; return cuda_fail(e, "cb_backward_kernel"); }
     }
     delete p;
+    if constexpr (std::is_same<T, float>::value) {
+        if (cw) return zfold(ws ? (const float *)ws : nullptr, vol, g->grid, s);
+    }
     if (tr) {
         dim3 grid((g->grid.nx + 31) / 32, (g->grid.ny + 31) / 32, g->grid.nz);
         fold_add_kernel<T><<<grid, dim3(32, 8), 0, s>>>((const T *)ws, vol, g->grid.nx, g->grid.ny);
@@ -611,12 +575,8 @@ static nefct_status cb_forward_static_impl(const nefct_cb_geom *g, const float *
     for (int v0 = 0; v0 < g->nv; v0 += ViewTable<float>::kMax) {
         const int nvc = std::min(ViewTable<float>::kMax, g->nv - v0);
         fill_views(p, g, v0, nvc);
-        dim3 grid, block;
-        cb_shape(p, g->na, g->nb, nvc, grid, block);
-        if (flags & NEFCT_EXACT) cb_forward_kernel<float, false, true><<<grid, block, 0, s>>>(p);
-        else if (cubic(p.g)) cb_forward_kernel<float, false><<<grid, block, 0, s>>>(p);
-        else cb_forward_kernel<float, true><<<grid, block, 0, s>>>(p);
-        NEFCT_CHECK_LAUNCH("cb_forward_kernel (noalloc)");
+        const cudaError_t e = cb_launch_forward<float>(p, g->na, g->nb, nvc, flags, s, false);
+        if (e != cudaSuccess) return cuda_fail(e, "cb_forward_kernel (noalloc)");
     }
     return NEFCT_OK;
 }

@@ -20,8 +20,8 @@
 //    so the clip changes no result, only the trip count;
 //  * the three-way case split is written as one predicated sequence of at
 //    most three (voxel, weight) slots, in the reference's accumulation order;
-//  * the crossing ratios use the fast division (<= 2 ulp) in FP32: they only
-//    scale weights, and the split is continuous in them;
+//  * the crossing ratios use the approximate reciprocal (<= 2 ulp) in FP32:
+//    they only scale weights, and the split is continuous in them;
 //  * the per-ray weight W is applied once to the ray's sum of value * ratio
 //    (rounding-level difference from the per-contribution products);
 //  * slabs whose candidate voxels are all inside the grid skip the range
@@ -188,10 +188,68 @@ __device__ __forceinline__ bool setup_walk(const GridDev<T> &g, const T *r, uint
     return w.k0 <= w.k1;
 }
 
+// Floors of plane positions.  FP32: floor(q) + 1.5*2^23 equals
+// round-down(q + 1.5*2^23) exactly for |q| < 2^22 (the sum lies in
+// [2^23, 2^24), where the float spacing is 1); the float floor is that sum
+// minus 1.5*2^23 (exact) and the integer floor its bit pattern minus
+// 0x4B400000, so no conversion instruction is needed.  Interior slabs have
+// positions inside the grid; boundary slabs clamp the positions to +-2^21
+// first (grid dimensions are limited to 2^20, so a clamped position stays
+// outside the grid and its voxels stay rejected).  FP64 converts.
+constexpr float kFloorMagic = 12582912.0f;   // 1.5 * 2^23
+constexpr int kFloorMagicBits = 0x4B400000;
+constexpr float kFloorClamp = 2097152.0f;    // 2^21
+
+template <bool CHECK> __device__ __forceinline__ float magic_floor(float q)
+{
+    if (CHECK) q = fminf(fmaxf(q, -kFloorClamp), kFloorClamp);
+    return __fadd_rd(q, kFloorMagic);
+}
+
+template <bool CHECK> __device__ __forceinline__ float2 magic_floor2(float2 q)
+{
+    if (CHECK) q = make_float2(fminf(fmaxf(q.x, -kFloorClamp), kFloorClamp), fminf(fmaxf(q.y, -kFloorClamp), kFloorClamp));
+    return __fadd2_rd(q, make_float2(kFloorMagic, kFloorMagic));
+}
+
+// Floor records M of a position: FP32 the biased float above, FP64 the int.
+//   value2(a, b)  the two floors as T;  biased(m)  floor + bias as unsigned;
+//   to_int(m)     the floor.
+template <typename T> struct Floor;
+template <> struct Floor<float> {
+    using M = float;
+    static constexpr unsigned kBias = (unsigned)kFloorMagicBits;
+    template <bool CHECK> static __device__ __forceinline__ void of2(Pair<float> q, M &a, M &b)
+    {
+        const float2 m = magic_floor2<CHECK>(q.v);
+        a = m.x; b = m.y;
+    }
+    static __device__ __forceinline__ Pair<float> value2(M a, M b)
+    {
+        Pair<float> p;
+        p.v = __fadd2_rn(make_float2(a, b), make_float2(-kFloorMagic, -kFloorMagic));
+        return p;
+    }
+    static __device__ __forceinline__ unsigned biased(M m) { return (unsigned)__float_as_int(m); }
+    static __device__ __forceinline__ int to_int(M m) { return __float_as_int(m) - kFloorMagicBits; }
+};
+template <> struct Floor<double> {
+    using M = int;
+    static constexpr unsigned kBias = 0u;
+    template <bool CHECK> static __device__ __forceinline__ void of2(Pair<double> q, M &a, M &b)
+    {
+        a = __double2int_rd(q.x());
+        b = __double2int_rd(q.y());
+    }
+    static __device__ __forceinline__ Pair<double> value2(M a, M b) { return Pair<double>::make((double)a, (double)b); }
+    static __device__ __forceinline__ unsigned biased(M m) { return (unsigned)m; }
+    static __device__ __forceinline__ int to_int(M m) { return m; }
+};
+
 // The up-to-three contributions of one driving slab: flat volume index,
 // split ratio r (the weight is r * W) and activity, in the reference's order.
 template <typename T> struct SlabSlots {
-    int idx[3];
+    unsigned idx[3];
     T r[3];
     bool ok[3];
     bool mid3;          // slot 1 is the middle entry of a three-voxel split (Q5)
@@ -201,19 +259,29 @@ template <typename T> struct SlabSlots {
 // the z row offsets from one slab to the next.
 //   DIV   the grid is not cubic: positions divide by dy (x-driven) / dz;
 //   SWP   the z slope is >= 0 (uniform along a detector row, so along a warp);
+//   VUP   the transverse slope kv is >= 0, so the v position grows along the
+//         walk (the entry plane is the low one; rounding is monotone, so this
+//         equals the reference's min/max choice);
 //   SV1   the transverse stride is 1 (x-fastest volume for y-driven rays,
-//         y-fastest copy for x-driven rays).
+//         y-fastest copy for x-driven rays);
+//   EXACT crossing ratios by exact division (the intersection count).
 // next<CHECK>() returns the next slab's contributions; CHECK=false is only
 // valid for interior slabs, where all candidate voxels are inside the grid.
-template <typename T, bool DIV, bool SWP, bool SV1, bool EXACT = false> struct Walker {
+// Indices are computed modulo 2^32 from biased floors; for admitted voxels
+// the biases cancel and the index is exact.
+template <typename T, bool DIV, bool SWP, bool VUP, bool SV1, bool EXACT = false> struct Walker {
     using F = FP<T>;
     using P2 = Pair<T>;
+    using FL = Floor<T>;
+    using M = typename FL::M;
     P2 p0, k2, n2;          // (pv, pw), (kv, kw), (nv2, nz2)
     T pu, dv, dz;
-    int nv, nz, su, sv, sw, base;
+    int nv, nz, su, sv, sw;
+    unsigned base;          // k * su minus the floors' biases
     bool vdiv, zdiv;
     T t, qav, qaw;
-    int fav, faw, rowa;
+    M mav, maw;
+    unsigned rowa;
 
     // Positions of plane t in v and z: ((p + k * (t - pu)) [/ d]) + n/2, the
     // reference's order (:54-55, :67-68, :194-195, :207-208), both axes at once.
@@ -235,14 +303,13 @@ template <typename T, bool DIV, bool SWP, bool SV1, bool EXACT = false> struct W
         nv = w.nv; nz = g.nz; su = su_; sv = SV1 ? 1 : sv_; sw = sw_;
         vdiv = w.vdiv;
         zdiv = dz != (T)1;
-        base = k * su;
+        base = (unsigned)k * (unsigned)su - FL::kBias * ((unsigned)sv + (unsigned)sw);
         t = F::sub((T)k, w.nu2);
         const P2 q = pos(t);
         qav = q.x();
         qaw = q.y();
-        fav = F::ifloor(qav);
-        faw = F::ifloor(qaw);
-        rowa = faw * sw;
+        FL::template of2<true>(q, mav, maw);
+        rowa = FL::biased(maw) * (unsigned)sw;
     }
 
     template <bool CHECK> __device__ __forceinline__ SlabSlots<T> next()
@@ -250,36 +317,39 @@ template <typename T, bool DIV, bool SWP, bool SV1, bool EXACT = false> struct W
         const T t2 = F::add(t, (T)1);
         const P2 qb = pos(t2);
         const T qbv = qb.x(), qbw = qb.y();
-        const int fbv = F::ifloor(qbv), fbw = F::ifloor(qbw);
-        const int rowb = fbw * sw;
-        // low/high plane of the slab in v (min/max equals the slope-sign choice)
-        const T q1v = F::min(qav, qbv), q2v = F::max(qav, qbv);
-        const int cv1 = min(fav, fbv), cv2 = max(fav, fbv);
+        M mbv, mbw;
+        FL::template of2<CHECK>(qb, mbv, mbw);
+        const unsigned rowb = FL::biased(mbw) * (unsigned)sw;
+        // low/high plane of the slab in v and z (static by the slope signs)
+        const T q1v = VUP ? qav : qbv, q2v = VUP ? qbv : qav;
+        const M m1v = VUP ? mav : mbv, m2v = VUP ? mbv : mav;
         const T q1w = SWP ? qaw : qbw, q2w = SWP ? qbw : qaw;
-        const int cw1 = SWP ? faw : fbw, cw2 = SWP ? fbw : faw;
-        const int row1 = SWP ? rowa : rowb, row2 = SWP ? rowb : rowa;
-        const int b = base;
-        t = t2; qav = qbv; qaw = qbw; fav = fbv; faw = fbw; rowa = rowb; base += su;
+        const M m1w = SWP ? maw : mbw, m2w = SWP ? mbw : maw;
+        const unsigned row1 = SWP ? rowa : rowb, row2 = SWP ? rowb : rowa;
+        const unsigned b = base;
+        t = t2; qav = qbv; qaw = qbw; mav = mbv; maw = mbw; rowa = rowb; base += (unsigned)su;
 
-        const bool vx = cv1 != cv2, wx = cw1 != cw2;
+        const bool vx = m1v != m2v, wx = m1w != m2w;
         // crossing ratios (c2 - q1) / (q2 - q1) of both axes (reference :94, :118, :134-135)
         const P2 nq1 = P2::make(-q1v, -q1w);
-        const P2 num = P2::add(P2::make((T)cv2, (T)cw2), nq1);
+        const P2 num = P2::add(FL::value2(m2v, m2w), nq1);
         const P2 den = P2::add(P2::make(q2v, q2w), nq1);
         const T rvq = EXACT ? F::div(num.x(), den.x()) : F::ratio(num.x(), den.x());
         const T rwq = EXACT ? F::div(num.y(), den.y()) : F::ratio(num.y(), den.y());
         const T rv = vx ? rvq : (T)1, rw = wx ? rwq : (T)1;
         const bool vfirst = rv > rw;   // middle voxel (cv1, cw2) when true, else (cv2, cw1)
+        const unsigned V1 = FL::biased(m1v) * (unsigned)sv, V2 = FL::biased(m2v) * (unsigned)sv;
         SlabSlots<T> s;
         s.r[0] = F::min(rv, rw);
         s.r[1] = F::abs(F::sub(rv, rw));
         s.r[2] = F::sub((T)1, F::max(rv, rw));
-        s.idx[0] = b + cv1 * sv + row1;
-        s.idx[1] = b + (vfirst ? cv1 * sv + row2 : cv2 * sv + row1);
-        s.idx[2] = b + cv2 * sv + row2;
+        s.idx[0] = b + V1 + row1;
+        s.idx[1] = b + (vfirst ? V1 + row2 : V2 + row1);
+        s.idx[2] = b + V2 + row2;
         s.mid3 = vx && wx;
         if (CHECK) {
             // slab admission (reference :80, :92, :112, :116, :132)
+            const int cv1 = FL::to_int(m1v), cv2 = FL::to_int(m2v), cw1 = FL::to_int(m1w), cw2 = FL::to_int(m2w);
             const bool adm = (unsigned)(cv1 + (int)vx) < (unsigned)(nv + (int)vx) &&
                              (unsigned)(cw1 + (int)wx) < (unsigned)(nz + (int)wx);
             const int mv = vfirst ? cv1 : cv2, mw = vfirst ? cw2 : cw1;
@@ -318,13 +388,25 @@ __device__ __forceinline__ void walk_all(WK &it, const int k0, const int k1, con
     }
 }
 
+// Calls body(Walker<...>) with the walker variant of the ray's slope signs.
+template <typename T, bool DIV, bool SV1, bool EXACT = false, class Body>
+__device__ __forceinline__ void with_walker(const Walk<T> &w, const GridDev<T> &g, int su, int sv, int sw, Body &&body)
+{
+    if (w.kw >= (T)0) {
+        if (w.kv >= (T)0) { Walker<T, DIV, true, true, SV1, EXACT> it(w, g, w.k0, su, sv, sw); body(it); }
+        else { Walker<T, DIV, true, false, SV1, EXACT> it(w, g, w.k0, su, sv, sw); body(it); }
+    } else {
+        if (w.kv >= (T)0) { Walker<T, DIV, false, true, SV1, EXACT> it(w, g, w.k0, su, sv, sw); body(it); }
+        else { Walker<T, DIV, false, false, SV1, EXACT> it(w, g, w.k0, su, sv, sw); body(it); }
+    }
+}
+
 // Weighted sum of the volume along the ray (forward):
 //   sum over contributions of v * r, times W (and Wmid for Q5 middles).
-template <typename T, bool DIV, bool SWP, bool SV1, bool Q5>
-__device__ __forceinline__ T gather_walk_t(const Walk<T> &w, const GridDev<T> &g, const T *__restrict__ base,
-                                           int su, int sv, int sw)
+template <typename T, bool DIV, bool SV1, bool Q5>
+__device__ __forceinline__ T gather_walk(const Walk<T> &w, const GridDev<T> &g, const T *__restrict__ base, int su,
+                                         int sv, int sw)
 {
-    Walker<T, DIV, SWP, SV1> it(w, g, w.k0, su, sv, sw);
     T acc = (T)0, accm = (T)0;
     auto f = [&](const SlabSlots<T> &s) {
         const T v0 = s.ok[0] ? __ldg(base + s.idx[0]) : (T)0;
@@ -335,40 +417,23 @@ __device__ __forceinline__ T gather_walk_t(const Walk<T> &w, const GridDev<T> &g
         else acc += v1 * s.r[1];
         acc += v2 * s.r[2];
     };
-    walk_all(it, w.k0, w.k1, w.ki0, w.ki1, f);
+    with_walker<T, DIV, SV1>(w, g, su, sv, sw, [&](auto &it) { walk_all(it, w.k0, w.k1, w.ki0, w.ki1, f); });
     return Q5 ? acc * w.W + accm * w.Wmid : acc * w.W;
-}
-
-template <typename T, bool DIV, bool SV1, bool Q5>
-__device__ __forceinline__ T gather_walk(const Walk<T> &w, const GridDev<T> &g, const T *__restrict__ base, int su,
-                                         int sv, int sw)
-{
-    return w.kw >= (T)0 ? gather_walk_t<T, DIV, true, SV1, Q5>(w, g, base, su, sv, sw)
-                        : gather_walk_t<T, DIV, false, SV1, Q5>(w, g, base, su, sv, sw);
 }
 
 // Scatters value * weight along the ray (transpose); reductions do not wait
 // for their result.
-template <typename T, bool DIV, bool SWP, bool SV1, bool Q5>
-__device__ __forceinline__ void scatter_walk_t(const Walk<T> &w, const GridDev<T> &g, T *base, int su, int sv,
-                                               int sw, T value)
+template <typename T, bool DIV, bool SV1, bool Q5>
+__device__ __forceinline__ void scatter_walk(const Walk<T> &w, const GridDev<T> &g, T *base, int su, int sv, int sw,
+                                             T value)
 {
-    Walker<T, DIV, SWP, SV1> it(w, g, w.k0, su, sv, sw);
     const T yw = value * w.W, ym = value * w.Wmid;
     auto f = [&](const SlabSlots<T> &s) {
         if (s.ok[0]) atomicAdd(base + s.idx[0], yw * s.r[0]);
         if (s.ok[1]) atomicAdd(base + s.idx[1], ((Q5 && s.mid3) ? ym : yw) * s.r[1]);
         if (s.ok[2]) atomicAdd(base + s.idx[2], yw * s.r[2]);
     };
-    walk_all(it, w.k0, w.k1, w.ki0, w.ki1, f);
-}
-
-template <typename T, bool DIV, bool SV1, bool Q5>
-__device__ __forceinline__ void scatter_walk(const Walk<T> &w, const GridDev<T> &g, T *base, int su, int sv, int sw,
-                                             T value)
-{
-    if (w.kw >= (T)0) scatter_walk_t<T, DIV, true, SV1, Q5>(w, g, base, su, sv, sw, value);
-    else scatter_walk_t<T, DIV, false, SV1, Q5>(w, g, base, su, sv, sw, value);
+    with_walker<T, DIV, SV1>(w, g, su, sv, sw, [&](auto &it) { walk_all(it, w.k0, w.k1, w.ki0, w.ki1, f); });
 }
 
 // Deterministic transpose: each contribution value * weight is scaled by
@@ -378,26 +443,17 @@ __device__ __forceinline__ void scatter_walk(const Walk<T> &w, const GridDev<T> 
 __device__ __forceinline__ long long to_fixed(float v) { return __float2ll_rn(v); }
 __device__ __forceinline__ long long to_fixed(double v) { return __double2ll_rn(v); }
 
-template <typename T, bool DIV, bool SWP, bool SV1>
-__device__ __forceinline__ void scatter_walk_fixed_t(const Walk<T> &w, const GridDev<T> &g, unsigned long long *base,
-                                                     int su, int sv, int sw, T value, T scale)
+template <typename T, bool DIV, bool SV1>
+__device__ __forceinline__ void scatter_walk_fixed(const Walk<T> &w, const GridDev<T> &g, unsigned long long *base,
+                                                   int su, int sv, int sw, T value, T scale)
 {
-    Walker<T, DIV, SWP, SV1> it(w, g, w.k0, su, sv, sw);
     const T yw = value * w.W;
     auto f = [&](const SlabSlots<T> &s) {
 #pragma unroll
         for (int j = 0; j < 3; ++j)
             if (s.ok[j]) atomicAdd(base + s.idx[j], (unsigned long long)to_fixed((yw * s.r[j]) * scale));
     };
-    walk_all(it, w.k0, w.k1, w.ki0, w.ki1, f);
-}
-
-template <typename T, bool DIV, bool SV1>
-__device__ __forceinline__ void scatter_walk_fixed(const Walk<T> &w, const GridDev<T> &g, unsigned long long *base,
-                                                   int su, int sv, int sw, T value, T scale)
-{
-    if (w.kw >= (T)0) scatter_walk_fixed_t<T, DIV, true, SV1>(w, g, base, su, sv, sw, value, scale);
-    else scatter_walk_fixed_t<T, DIV, false, SV1>(w, g, base, su, sv, sw, value, scale);
+    with_walker<T, DIV, SV1>(w, g, su, sv, sw, [&](auto &it) { walk_all(it, w.k0, w.k1, w.ki0, w.ki1, f); });
 }
 
 // Number of contributions of the ray (the throughput unit).  Uses the
@@ -408,13 +464,7 @@ __device__ __forceinline__ unsigned count_walk(const Walk<T> &w, const GridDev<T
 {
     unsigned n = 0;
     auto f = [&](const SlabSlots<T> &s) { n += (unsigned)s.ok[0] + (unsigned)s.ok[1] + (unsigned)s.ok[2]; };
-    if (w.kw >= (T)0) {
-        Walker<T, DIV, true, true, true> it(w, g, w.k0, 0, 1, 0);
-        walk_all(it, w.k0, w.k1, w.ki0, w.ki1, f);
-    } else {
-        Walker<T, DIV, false, true, true> it(w, g, w.k0, 0, 1, 0);
-        walk_all(it, w.k0, w.k1, w.ki0, w.ki1, f);
-    }
+    with_walker<T, DIV, true, true>(w, g, 0, 1, 0, [&](auto &it) { walk_all(it, w.k0, w.k1, w.ki0, w.ki1, f); });
     return n;
 }
 

@@ -12,6 +12,18 @@ from tests.test_gpu_siddon import assert_parity
 pytestmark = pytest.mark.gpu
 
 
+def _thread_walk_forward(v, g, flags=0):
+    """Per-problem forward with the thread-per-ray walk, the per-ray code the
+    batch kernels share (bitwise comparable)."""
+    from nefct_b200 import autotune
+    saved = autotune.current()
+    try:
+        autotune.apply(saved["rows"], saved["order"], 0)
+        return ops.cb_forward(v, g, flags)
+    finally:
+        autotune.apply(saved["rows"], saved["order"], saved["walk"])
+
+
 def _problems(dev):
     rng = np.random.default_rng(4)
     geoms = [
@@ -39,7 +51,7 @@ def test_batch_matches_per_problem(cuda, flags, strategy):
     bp.step()
     torch.cuda.synchronize()
     for g, v, gr, s, b in zip(geoms, vols, grads, bp.sinos, bp.backs):
-        ref = ops.cb_forward(v, g, flags)
+        ref = _thread_walk_forward(v, g, flags)
         assert torch.equal(s, ref)                       # same per-ray code: bitwise
         assert_parity(b.cpu().numpy(), ops.cb_backward(gr, g, flags).cpu().numpy())
 
@@ -57,7 +69,7 @@ def test_batch_graph_replay(cuda, strategy):
     graph.replay()
     torch.cuda.synchronize()
     for g, v, gr, s, b in zip(geoms, vols, grads, bp.sinos, bp.backs):
-        assert torch.equal(s, ops.cb_forward(v, g))
+        assert torch.equal(s, _thread_walk_forward(v, g))
         assert_parity(b.cpu().numpy(), ops.cb_backward(gr, g).cpu().numpy())
     assert bp.tiles > 0
 

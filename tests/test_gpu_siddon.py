@@ -216,25 +216,62 @@ def test_linearity_and_adjoint_config2_size(cuda):
 
 
 def test_launch_shapes_give_identical_forward(cuda):
-    """Every autotuner variant runs the same per-ray arithmetic: the forward
-    is bitwise identical across rows-per-CTA and grid orders."""
+    """Launch shapes do not change the per-ray arithmetic: the forward is
+    bitwise identical across rows (columns) per CTA and grid orders for each
+    walk, and the two walks (thread per ray, column warps) agree to float
+    rounding of the accumulation.  The geometry has a partial last row tile
+    (45 rows) and row tiles that straddle the central row (z slopes of both
+    signs in one warp); the transpose gets zero rays inside a warp.  The
+    transpose agrees to float rounding (atomic summation order)."""
     from nefct_b200 import autotune
     g = nb.ConeBeam((40, 36, 30), np.linspace(0, 2 * np.pi, 33, endpoint=False), 150.0, 300.0, 70, 1.3, 45, 1.1,
                     size=(40.0, 36.0, 30.0))
-    vol = torch.rand(g.vol_shape, device=cuda, generator=torch.Generator(device=cuda).manual_seed(8))
+    gen = torch.Generator(device=cuda).manual_seed(8)
+    vol = torch.rand(g.vol_shape, device=cuda, generator=gen)
+    y = torch.rand(g.sino_shape, device=cuda, generator=gen)
+    y[3, 10:14] = 0
+    y[5, :, 7] = 0
     saved = autotune.current()
     try:
-        outs = []
+        outs, backs = {}, []
         for rows in (1, 2, 4, 8):
             for order in (0, 1):
-                autotune.apply(rows, order)
-                outs.append(ops.cb_forward(vol, g).cpu())
-        for o in outs[1:]:
-            assert torch.equal(o, outs[0])
+                for walk in (0, 3):
+                    autotune.apply(rows, order, walk)
+                    outs.setdefault(walk, []).append(ops.cb_forward(vol, g).cpu())
+                    backs.append(ops.cb_backward(y, g).cpu().double())
+        for walk, group in outs.items():
+            for i, o in enumerate(group[1:]):
+                assert torch.equal(o, group[0]), f"walk {walk} variant {i + 1}"
+        ref = outs[0][0].double()
+        assert float((outs[3][0].double() - ref).norm() / ref.norm()) < 1e-6
+        for b in backs[1:]:
+            assert float((b - backs[0]).norm() / backs[0].norm()) < 1e-6
         rec = autotune.tune_cone_beam(g, 0, cuda, reps=1, use_cache=False)
-        assert rec["rows"] in (2, 4, 8) and rec["order"] in (0, 1) and len(rec["ms"]) == 6
+        assert rec["rows"] in (2, 4, 8) and rec["order"] in (0, 1) and rec["walk"] in (0, 1, 2, 3)
+        assert len(rec["ms"]) == 12
     finally:
-        autotune.apply(saved["rows"], saved["order"])
+        autotune.apply(saved["rows"], saved["order"], saved["walk"])
+
+
+@pytest.mark.parametrize("walk", [0, 3])
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_walks_vs_reference(cuda, golden, case, walk):
+    """Forward and reference backprojection (incl. Q8 for the cylindrical
+    case) with both walks against the reference fixtures."""
+    from nefct_b200 import autotune
+    name, grid, centre, size, cyl, da = case
+    g = _geom(case, golden["angles"])
+    saved = autotune.current()
+    try:
+        autotune.apply(saved["rows"], saved["order"], walk)
+        out = ops.cb_forward(torch.from_numpy(golden[f"{name}/vol"]).to(cuda), g).cpu().numpy()
+        assert_parity(out, golden[f"{name}/fwd"])
+        bp = ops.cb_backward(torch.from_numpy(golden[f"{name}/sino_in"]).to(cuda), g,
+                             _lib.REF_BACKPROJECT | (_lib.Q8_INDEX if cyl else 0)).cpu().numpy()
+        assert_parity(bp, golden[f"{name}/bp"])
+    finally:
+        autotune.apply(saved["rows"], saved["order"], saved["walk"])
 
 
 @pytest.mark.parametrize("flags", [0, _lib.LINE_INTEGRAL, _lib.REF_BACKPROJECT, _lib.NO_TRANSPOSE])

@@ -135,25 +135,24 @@ __global__ void __launch_bounds__(256) cb_colwarp_kernel(const __grid_constant__
     if (FWD) {
         const float *__restrict__ src = p.volT;
         float acc = 0.f;
-        auto f = [&](const SlabSlots<float> &s) {
-            const float v0 = s.ok[0] ? __ldg(src + s.idx[0]) : 0.f;
-            const float v1 = s.ok[1] ? __ldg(src + s.idx[1]) : 0.f;
-            const float v2 = s.ok[2] ? __ldg(src + s.idx[2]) : 0.f;
-            acc += v0 * s.r[0];
-            acc += v1 * s.r[1];
-            acc += v2 * s.r[2];
+        auto f = [&](const auto &s) {
+            float v[s.n];
+#pragma unroll
+            for (int i = 0; i < s.n; ++i) v[i] = s.ok[i] ? __ldg(src + s.idx[i]) : 0.f;
+#pragma unroll
+            for (int i = 0; i < s.n; ++i) acc += v[i] * s.r[i];
         };
-        col_walk_any<DIV>(c, L, K0, K1, KI0, KI1, p.g, f);
+        col_walk_any<DIV, false>(c, L, K0, K1, KI0, KI1, p.g, f);
         if (has) *sino_out = live ? acc * w.W : 0.f;
     } else {
         float *dst = p.outT;
         const float yw = y * w.W;
-        auto f = [&](const SlabSlots<float> &s) {
-            if (s.ok[0]) atomicAdd(dst + s.idx[0], yw * s.r[0]);
-            if (s.ok[1]) atomicAdd(dst + s.idx[1], yw * s.r[1]);
-            if (s.ok[2]) atomicAdd(dst + s.idx[2], yw * s.r[2]);
+        auto f = [&](const auto &s) {
+#pragma unroll
+            for (int i = 0; i < s.n; ++i)
+                if (s.ok[i]) atomicAdd(dst + s.idx[i], yw * s.r[i]);
         };
-        col_walk_any<DIV>(c, L, K0, K1, KI0, KI1, p.g, f);
+        col_walk_any<DIV, true>(c, L, K0, K1, KI0, KI1, p.g, f);
     }
 }
 

@@ -11,7 +11,9 @@
 // union of their slab ranges:
 //  * the v part of each slab is computed once per warp: lane j builds the
 //    entry of slab kc + j of a 32-slab chunk, and each slab's entry is
-//    broadcast with shuffles (3 per interior slab, 4 per boundary slab);
+//    broadcast with shuffles; whether the slab crosses a v plane is the same
+//    for the whole warp, so the common case without a crossing takes a
+//    two-slot split without divergence;
 //  * each lane evaluates the z part and the three-voxel split of its own
 //    ray exactly as the single-ray walker does (same operations, same order);
 //  * the volume (forward) and the accumulator (transpose) are z-fastest
@@ -79,15 +81,29 @@ struct ColLane {
     bool live, up;
 };
 
+// Contributions of one slab of a lane's ray: NS slots (voxel index, split
+// ratio, activity) in the reference's accumulation order.
+template <int NS> struct ColSlots {
+    static constexpr int n = NS;
+    unsigned idx[NS];
+    float r[NS];
+    bool ok[NS];
+};
+
 // One slab of the lane's ray.  WUP: 1 every live ray has kw >= 0, 0 every
-// live ray has kw < 0, 2 mixed (per-lane choice).
-template <bool DIV, bool CHECK, int WUP>
-__device__ __forceinline__ SlabSlots<float> col_slab(ColLane &L, float d, float dz, bool zdiv, float nz2, int nv,
-                                                     int nz, const ColEntry &e, int j)
+// live ray has kw < 0, 2 mixed (per-lane choice).  The v crossing is shared
+// by the warp (b1 != b2): without one (VX false) the split has two slots,
+// (v1, w1) with ratio rw and (v1, w2) with 1 - rw, which is the general
+// three-slot split with rv = 1 (its third ratio, 1 - max(rv, rw), is 0 and
+// its slot inactive); with one, the general split.  SPLIT false takes the
+// general split for every slab (no branch: the forward's loads of
+// consecutive slabs interleave better).  f(slots) consumes.
+template <bool DIV, bool CHECK, int WUP, bool SPLIT, class Fn>
+__device__ __forceinline__ void col_slab(ColLane &L, float d, float dz, bool zdiv, float nz2, int nv, int nz,
+                                         const ColEntry &e, int j, Fn &f)
 {
     const unsigned b1 = __shfl_sync(0xffffffffu, e.b1, j);
     const unsigned b2 = __shfl_sync(0xffffffffu, e.b2, j);
-    const float rv = __shfl_sync(0xffffffffu, e.rv, j);
     unsigned cv = 0;
     if (CHECK) cv = __shfl_sync(0xffffffffu, e.cv, j);
 
@@ -100,39 +116,60 @@ __device__ __forceinline__ SlabSlots<float> col_slab(ColLane &L, float d, float 
     const float m1w = up ? L.maw : mbw, m2w = up ? mbw : L.maw;
     L.qaw = qbw;
     L.maw = mbw;
-    const bool vx = b1 != b2, wx = m1w != m2w;
+    const bool wx = m1w != m2w;
     const float rw = wx ? FP<float>::ratio(__fadd_rn(__fadd_rn(m2w, -kFloorMagic), -q1w), __fadd_rn(q2w, -q1w)) : 1.f;
-    const bool vfirst = rv > rw;
     const unsigned i1 = (unsigned)__float_as_int(m1w), i2 = (unsigned)__float_as_int(m2w);
-    SlabSlots<float> s;
-    s.r[0] = fminf(rv, rw);
-    s.r[1] = fabsf(__fsub_rn(rv, rw));
-    s.r[2] = __fsub_rn(1.f, fmaxf(rv, rw));
-    s.idx[0] = b1 + i1;
-    s.idx[1] = vfirst ? b1 + i2 : b2 + i1;
-    s.idx[2] = b2 + i2;
-    s.mid3 = vx && wx;
-    if (CHECK) {
-        // slab admission (reference siddon.cu.cc :80, :92, :112, :116, :132)
-        const int cv1 = (int)(cv & 0xffffu) - 2, cv2 = (int)(cv >> 16) - 2;
-        const int cw1 = (int)i1 - kFloorMagicBits, cw2 = (int)i2 - kFloorMagicBits;
-        const bool adm = L.live && (unsigned)(cv1 + (int)vx) < (unsigned)(nv + (int)vx) &&
-                         (unsigned)(cw1 + (int)wx) < (unsigned)(nz + (int)wx);
-        const int mv = vfirst ? cv1 : cv2, mw = vfirst ? cw2 : cw1;
-        s.ok[0] = adm && (cv1 | cw1) >= 0;
-        s.ok[1] = adm && (vx || wx) && (unsigned)mv < (unsigned)nv && (unsigned)mw < (unsigned)nz;
-        s.ok[2] = adm && vx && wx && cv2 < nv && cw2 < nz;
+    const int cv1 = CHECK ? (int)(cv & 0xffffu) - 2 : 0, cv2 = CHECK ? (int)(cv >> 16) - 2 : 0;
+    const int cw1 = (int)i1 - kFloorMagicBits, cw2 = (int)i2 - kFloorMagicBits;
+    if (SPLIT && b1 == b2) {
+        // no v crossing (uniform across the warp)
+        const bool vfirst = 1.f > rw;
+        ColSlots<2> s;
+        s.r[0] = rw;                            // min(1, rw)
+        s.r[1] = __fsub_rn(1.f, rw);            // |1 - rw|
+        s.idx[0] = b1 + i1;
+        s.idx[1] = b1 + (vfirst ? i2 : i1);
+        if (CHECK) {
+            const bool adm = L.live && (unsigned)cv1 < (unsigned)nv && (unsigned)(cw1 + (int)wx) < (unsigned)(nz + (int)wx);
+            const int mw = vfirst ? cw2 : cw1;
+            s.ok[0] = adm && cw1 >= 0;
+            s.ok[1] = adm && wx && (unsigned)mw < (unsigned)nz;
+        } else {
+            s.ok[0] = L.live;
+            s.ok[1] = L.live && wx;
+        }
+        f(s);
     } else {
-        s.ok[0] = L.live;
-        s.ok[1] = L.live && (vx || wx);
-        s.ok[2] = L.live && vx && wx;
+        const float rv = __shfl_sync(0xffffffffu, e.rv, j);
+        const bool vx = SPLIT || b1 != b2;
+        const bool vfirst = rv > rw;
+        ColSlots<3> s;
+        s.r[0] = fminf(rv, rw);
+        s.r[1] = fabsf(__fsub_rn(rv, rw));
+        s.r[2] = __fsub_rn(1.f, fmaxf(rv, rw));
+        s.idx[0] = b1 + i1;
+        s.idx[1] = vfirst ? b1 + i2 : b2 + i1;
+        s.idx[2] = b2 + i2;
+        if (CHECK) {
+            // slab admission (reference siddon.cu.cc :80, :92, :112, :116, :132)
+            const bool adm = L.live && (unsigned)(cv1 + (int)vx) < (unsigned)(nv + (int)vx) &&
+                             (unsigned)(cw1 + (int)wx) < (unsigned)(nz + (int)wx);
+            const int mv = vfirst ? cv1 : cv2, mw = vfirst ? cw2 : cw1;
+            s.ok[0] = adm && (cv1 | cw1) >= 0;
+            s.ok[1] = adm && (vx || wx) && (unsigned)mv < (unsigned)nv && (unsigned)mw < (unsigned)nz;
+            s.ok[2] = adm && vx && wx && cv2 < nv && cw2 < nz;
+        } else {
+            s.ok[0] = L.live;
+            s.ok[1] = L.live && (vx || wx);
+            s.ok[2] = L.live && vx && wx;
+        }
+        f(s);
     }
-    return s;
 }
 
 // Walks slabs [a, b] (inside the current 32-slab chunk starting at kc) in
 // one check mode.  t is the entry plane k - nu2 of slab k, carried exactly.
-template <bool DIV, bool CHECK, int WUP, class Fn>
+template <bool DIV, bool CHECK, int WUP, bool SPLIT, class Fn>
 __device__ __forceinline__ void col_range(int a, int b, int kc, float &t, const ColShared &c, ColLane &L,
                                           const ColEntry &e, const GridDev<float> &g, Fn &f)
 {
@@ -141,13 +178,13 @@ __device__ __forceinline__ void col_range(int a, int b, int kc, float &t, const 
     for (int k = a; k <= b; ++k) {
         const float t2 = __fadd_rn(t, 1.f);
         t = t2;
-        f(col_slab<DIV, CHECK, WUP>(L, __fsub_rn(t2, c.pu), g.dz, zdiv, g.nz2, c.nv, g.nz, e, k - kc));
+        col_slab<DIV, CHECK, WUP, SPLIT>(L, __fsub_rn(t2, c.pu), g.dz, zdiv, g.nz2, c.nv, g.nz, e, k - kc, f);
     }
 }
 
 // Slabs [K0, K1] of the warp in 32-slab chunks (lane j builds the entry of
 // slab kc + j); boundary slabs outside [KI0, KI1] with range checks.
-template <bool DIV, int WUP, class Fn>
+template <bool DIV, int WUP, bool SPLIT, class Fn>
 __device__ __forceinline__ void col_walk(const ColShared &c, ColLane &L, int K0, int K1, int KI0, int KI1,
                                          const GridDev<float> &g, Fn &f)
 {
@@ -162,21 +199,21 @@ __device__ __forceinline__ void col_walk(const ColShared &c, ColLane &L, int K0,
     for (int kc = K0; kc <= K1; kc += 32) {
         const ColEntry e = col_entry<DIV>(c, kc + lane);
         const int ke = min(K1, kc + 31);
-        col_range<DIV, true, WUP>(kc, min(ke, KI0 - 1), kc, t, c, L, e, g, f);
-        col_range<DIV, false, WUP>(max(kc, KI0), min(ke, KI1), kc, t, c, L, e, g, f);
-        col_range<DIV, true, WUP>(max(kc, KI1 + 1), ke, kc, t, c, L, e, g, f);
+        col_range<DIV, true, WUP, SPLIT>(kc, min(ke, KI0 - 1), kc, t, c, L, e, g, f);
+        col_range<DIV, false, WUP, SPLIT>(max(kc, KI0), min(ke, KI1), kc, t, c, L, e, g, f);
+        col_range<DIV, true, WUP, SPLIT>(max(kc, KI1 + 1), ke, kc, t, c, L, e, g, f);
     }
 }
 
-template <bool DIV, class Fn>
+template <bool DIV, bool SPLIT, class Fn>
 __device__ __forceinline__ void col_walk_any(const ColShared &c, ColLane &L, int K0, int K1, int KI0, int KI1,
                                              const GridDev<float> &g, Fn &f)
 {
     const bool all_up = __all_sync(0xffffffffu, L.up || !L.live);
     const bool all_down = __all_sync(0xffffffffu, !L.up || !L.live);
-    if (all_up) col_walk<DIV, 1>(c, L, K0, K1, KI0, KI1, g, f);
-    else if (all_down) col_walk<DIV, 0>(c, L, K0, K1, KI0, KI1, g, f);
-    else col_walk<DIV, 2>(c, L, K0, K1, KI0, KI1, g, f);
+    if (all_up) col_walk<DIV, 1, SPLIT>(c, L, K0, K1, KI0, KI1, g, f);
+    else if (all_down) col_walk<DIV, 0, SPLIT>(c, L, K0, K1, KI0, KI1, g, f);
+    else col_walk<DIV, 2, SPLIT>(c, L, K0, K1, KI0, KI1, g, f);
 }
 
 // Strides of the z-fastest layout [y][x][z] along (u, v) of the drive axis.

@@ -135,10 +135,13 @@ __global__ void __launch_bounds__(256) cb_colwarp_kernel(const __grid_constant__
     if (FWD) {
         const float *__restrict__ src = p.volT;
         float acc = 0.f;
+        // interior slabs load every slot unpredicated: an inactive slot has
+        // ratio 0 and a valid index (so a volume holding +-inf may give NaN
+        // where the reference gives +-inf); lanes without a ray are discarded
         auto f = [&](const auto &s) {
             float v[s.n];
 #pragma unroll
-            for (int i = 0; i < s.n; ++i) v[i] = s.ok[i] ? __ldg(src + s.idx[i]) : 0.f;
+            for (int i = 0; i < s.n; ++i) v[i] = (!s.checked || s.ok[i]) ? __ldg(src + s.idx[i]) : 0.f;
 #pragma unroll
             for (int i = 0; i < s.n; ++i) acc += v[i] * s.r[i];
         };

@@ -82,9 +82,13 @@ struct ColLane {
 };
 
 // Contributions of one slab of a lane's ray: NS slots (voxel index, split
-// ratio, activity) in the reference's accumulation order.
-template <int NS> struct ColSlots {
+// ratio, activity) in the reference's accumulation order.  In an interior
+// slab (CHK false) every slot's index is a voxel of the grid, also for an
+// inactive slot (whose ratio is 0: it repeats an active slot's voxel) and
+// for a lane without a ray (whose z plane stays at nz/2).
+template <int NS, bool CHK> struct ColSlots {
     static constexpr int n = NS;
+    static constexpr bool checked = CHK;
     unsigned idx[NS];
     float r[NS];
     bool ok[NS];
@@ -124,7 +128,7 @@ __device__ __forceinline__ void col_slab(ColLane &L, float d, float dz, bool zdi
     if (SPLIT && b1 == b2) {
         // no v crossing (uniform across the warp)
         const bool vfirst = 1.f > rw;
-        ColSlots<2> s;
+        ColSlots<2, CHECK> s;
         s.r[0] = rw;                            // min(1, rw)
         s.r[1] = __fsub_rn(1.f, rw);            // |1 - rw|
         s.idx[0] = b1 + i1;
@@ -143,7 +147,7 @@ __device__ __forceinline__ void col_slab(ColLane &L, float d, float dz, bool zdi
         const float rv = __shfl_sync(0xffffffffu, e.rv, j);
         const bool vx = SPLIT || b1 != b2;
         const bool vfirst = rv > rw;
-        ColSlots<3> s;
+        ColSlots<3, CHECK> s;
         s.r[0] = fminf(rv, rw);
         s.r[1] = fabsf(__fsub_rn(rv, rw));
         s.r[2] = __fsub_rn(1.f, fmaxf(rv, rw));
@@ -250,8 +254,9 @@ __device__ __forceinline__ bool col_setup(const GridDev<float> &g, const Walk<fl
     K1 = __reduce_max_sync(0xffffffffu, live ? w.k1 : INT_MIN);
     KI0 = __reduce_max_sync(0xffffffffu, live ? w.ki0 : INT_MIN);
     KI1 = __reduce_min_sync(0xffffffffu, live ? w.ki1 : INT_MAX);
-    L.pw = w.pw;
-    L.kw = w.kw;
+    // a lane without a ray walks the plane z = nz/2 (indices stay in the grid)
+    L.pw = live ? w.pw : 0.f;
+    L.kw = live ? w.kw : 0.f;
     L.live = live;
     L.up = w.kw >= 0.f;
     return true;

@@ -288,10 +288,13 @@ def run_gpu(args):
     # roofline of the dominant op (forward or adjoint) on its algorithmic bytes
     peak, peak_kind = load_peaks()
     fwd_s, bwd_s = t_fwd / args.steps, t_bwd / args.steps
+    walk = tuned["walk"]
     if bwd_s >= fwd_s:
-        dom, dom_t, alg = "cb_backward_kernel", bwd_s, 8 * inter + 4 * rays
+        dom = "cb_colwarp_kernel<transpose>" if walk & 2 else "cb_backward_kernel"
+        dom_t, alg = bwd_s, 8 * inter + 4 * rays
     else:
-        dom, dom_t, alg = "cb_forward_kernel", fwd_s, 4 * inter + 4 * rays
+        dom = "cb_colwarp_kernel<forward>" if walk & 1 else "cb_forward_kernel"
+        dom_t, alg = fwd_s, 4 * inter + 4 * rays
     achieved = alg / dom_t / 1e9
     traffic = load_traffic().get(dom)
 

@@ -12,8 +12,10 @@
 //
 // A plan holds, for n problems (each with its own grid, views, detector and
 // scanner), a table of work tiles -- 32 detector columns x R rows of one
-// view -- ordered longest rays first (problems sorted by slab count, views
-// and row bands inside).  The persistent kernel runs one CTA per resident
+// view for the thread walk, R columns x 32 rows for column warps (the walk
+// is fixed at plan time from NEFCT_TUNE_CB_WALK: column warps when both
+// directions use them) -- ordered longest rays first (problems sorted by
+// slab count, views and row bands inside).  The persistent kernel runs one CTA per resident
 // slot; each CTA takes the next tile from an atomic ticket counter until the
 // table is exhausted.  Tickets never wait on anything, so the kernel cannot
 // hang; load balance across uneven problems comes from the dynamic dequeue
@@ -22,24 +24,27 @@
 // stream-ordered and capturable in a CUDA graph after nefct_cb_batch_bind.
 //
 // Device workspace (caller-owned), 256-byte aligned sections:
-//   counters[4] | view tables | per-problem y-fastest volume
+//   counters[4] | view tables | per-problem volume copy
 // (problem descriptors and tile offsets travel as kernel parameters)
-// The y-fastest copy holds the transposed volume during the forward and
-// the accumulator of x-driven rays during the transpose.
+// The copy (y-fastest for the thread walk, z-fastest for column warps)
+// holds the transposed volume during the forward and the accumulator during
+// the transpose.
 #include <algorithm>
 #include <numeric>
 #include <string>
 #include <vector>
 
-#include "siddon.cuh"
+#include "cb_kernels.cuh"
 
 namespace nefct {
 
 nefct_status check_cb_geom(const nefct_cb_geom *g);
 nefct_status cb_forward_launches(const nefct_cb_geom *g, const float *vol, const float *volT, float *sino,
-                                 uint32_t flags, cudaStream_t s);
+                                 uint32_t flags, cudaStream_t s, bool colwarp);
 nefct_status cb_backward_launches(const nefct_cb_geom *g, const float *sino, float *out, float *outT,
-                                  uint32_t flags, cudaStream_t s);
+                                  uint32_t flags, cudaStream_t s, bool colwarp);
+nefct_status zmajor_copy(const float *in, float *out, const nefct_grid &g, cudaStream_t s);
+nefct_status zfold(const float *acc, float *vol, const nefct_grid &g, cudaStream_t s);
 
 struct BatchDesc {
     GridDev<float> g;
@@ -51,7 +56,7 @@ struct BatchDesc {
     float *sino;
     const float *grad;
     float *back;
-    float *volT;                         // y-fastest copy / accumulator
+    float *volT;                         // y- or z-fastest copy / accumulator
 };
 
 // Descriptors and tile offsets travel in the kernel parameter space (read
@@ -70,6 +75,7 @@ struct BatchPlan {
     std::vector<nefct_cb_problem> probs;   // caller order; geom.angles/z_offsets point into the copies below
     std::vector<std::vector<float>> angles, offsets;
     int strategy = NEFCT_BATCH_PER_PROBLEM;
+    bool colwarp = false;                  // column warps (fixed at plan time)
     std::vector<int> order;                // plan order -> caller index
     std::vector<BatchDesc> desc;           // plan order (device pointers filled at bind)
     std::vector<long long> t0;             // tile offsets, n + 1
@@ -133,6 +139,36 @@ __global__ void __launch_bounds__(256) batch_kernel(const __grid_constant__ Batc
     }
 }
 
+// Column-warp variant: a tile is blockDim.y columns x 32 rows of one view,
+// one warp per column.
+template <bool FWD, bool DIV>
+__global__ void __launch_bounds__(256) batch_colwarp_kernel(const __grid_constant__ BatchArgs a)
+{
+    __shared__ long long s_item;
+    for (;;) {
+        if (threadIdx.x == 0 && threadIdx.y == 0) s_item = a.begin + (long long)atomicAdd(a.counter, 1ull);
+        __syncthreads();
+        const long long item = s_item;
+        __syncthreads();                  // all threads read s_item before the next ticket
+        if (item >= a.end) return;        // uniform across the CTA
+        const int p = find_problem(a.t0, a.n, item);
+        const BatchDesc &P = a.d[p];
+        const long long local = item - a.t0[p];
+        const int ct = (int)(local % P.tiles_a);
+        const long long rest = local / P.tiles_a;
+        const int rt = (int)(rest % P.tiles_b);
+        const int iv = (int)(rest / P.tiles_b);
+        const int ia = ct * blockDim.y + threadIdx.y, ib = rt * 32 + threadIdx.x;
+        if (ia >= P.na) continue;         // uniform across the warp
+        const bool has = ib < P.nb;
+        const size_t id = ((size_t)iv * P.nb + (has ? ib : 0)) * P.na + ia;
+        float r[6];
+        cb_ray(P.rg, P.cs[iv], P.sn[iv], P.off[iv], ia, has ? ib : 0, r);
+        if (FWD) colwarp_lane<DIV, true>(P.g, r, has, P.flags, P.volT, P.sino + id, 0.f, nullptr);
+        else colwarp_lane<DIV, false>(P.g, r, has, P.flags, nullptr, nullptr, has ? P.grad[id] : 0.f, P.volT);
+    }
+}
+
 // Per-problem strategy: the single-problem kernels launched once per problem
 // (their scanner constants as kernel parameters), stream-ordered.
 static nefct_status batch_per_problem(BatchPlan *b, bool fwd, cudaStream_t s)
@@ -144,14 +180,23 @@ static nefct_status batch_per_problem(BatchPlan *b, bool fwd, cudaStream_t s)
         const size_t nvox = (size_t)D.g.nx * D.g.ny * D.g.nz;
         dim3 tg((D.g.nx + 31) / 32, (D.g.ny + 31) / 32, D.g.nz);
         nefct_status st;
-        if (fwd) {
+        if (b->colwarp) {
+            if (fwd) {
+                st = zmajor_copy(D.vol, D.volT, g.grid, s);
+                if (!st) st = cb_forward_launches(&g, D.vol, D.volT, D.sino, D.flags, s, true);
+            } else {
+                NEFCT_CHECK_CUDA(cudaMemsetAsync(D.volT, 0, nvox * sizeof(float), s));
+                st = cb_backward_launches(&g, D.grad, D.back, D.volT, D.flags, s, true);
+                if (!st) st = zfold(D.volT, D.back, g.grid, s);
+            }
+        } else if (fwd) {
             transpose_xy_kernel<float><<<tg, dim3(32, 8), 0, s>>>(D.vol, D.volT, D.g.nx, D.g.ny);
             NEFCT_CHECK_LAUNCH("transpose_xy_kernel (batch)");
-            st = cb_forward_launches(&g, D.vol, D.volT, D.sino, D.flags, s);
+            st = cb_forward_launches(&g, D.vol, D.volT, D.sino, D.flags, s, false);
         } else {
             NEFCT_CHECK_CUDA(cudaMemsetAsync(D.back, 0, nvox * sizeof(float), s));
             NEFCT_CHECK_CUDA(cudaMemsetAsync(D.volT, 0, nvox * sizeof(float), s));
-            st = cb_backward_launches(&g, D.grad, D.back, D.volT, D.flags, s);
+            st = cb_backward_launches(&g, D.grad, D.back, D.volT, D.flags, s, false);
             if (!st) {
                 fold_add_kernel<float><<<tg, dim3(32, 8), 0, s>>>(D.volT, D.back, D.g.nx, D.g.ny);
                 NEFCT_CHECK_LAUNCH("fold_add_kernel (batch)");
@@ -171,13 +216,17 @@ static nefct_status batch_launch(BatchPlan *b, bool fwd, cudaStream_t s)
     NEFCT_CHECK_CUDA(cudaMemsetAsync(counter, 0, 2 * sizeof(unsigned long long), s));
     for (int i = 0; i < n; ++i) {
         const BatchDesc &D = b->desc[i];
+        const nefct_cb_geom &g = b->probs[b->order[i]].geom;
         const size_t nvox = (size_t)D.g.nx * D.g.ny * D.g.nz;
         dim3 tg((D.g.nx + 31) / 32, (D.g.ny + 31) / 32, D.g.nz);
-        if (fwd) {
+        if (fwd && b->colwarp) {
+            nefct_status st = zmajor_copy(D.vol, D.volT, g.grid, s);
+            if (st) return st;
+        } else if (fwd) {
             transpose_xy_kernel<float><<<tg, dim3(32, 8), 0, s>>>(D.vol, D.volT, D.g.nx, D.g.ny);
             NEFCT_CHECK_LAUNCH("transpose_xy_kernel (batch)");
         } else {
-            NEFCT_CHECK_CUDA(cudaMemsetAsync(D.back, 0, nvox * sizeof(float), s));
+            if (!b->colwarp) NEFCT_CHECK_CUDA(cudaMemsetAsync(D.back, 0, nvox * sizeof(float), s));
             NEFCT_CHECK_CUDA(cudaMemsetAsync(D.volT, 0, nvox * sizeof(float), s));
         }
     }
@@ -186,19 +235,34 @@ static nefct_status batch_launch(BatchPlan *b, bool fwd, cudaStream_t s)
     BatchArgs &a = *b->args;
     if (b->split > 0) {
         a.begin = 0; a.end = b->split; a.counter = counter;
-        if (fwd) batch_kernel<true, false><<<b->grid_blocks, blk, 0, s>>>(a);
-        else batch_kernel<false, false><<<b->grid_blocks, blk, 0, s>>>(a);
+        if (b->colwarp) {
+            if (fwd) batch_colwarp_kernel<true, false><<<b->grid_blocks, blk, 0, s>>>(a);
+            else batch_colwarp_kernel<false, false><<<b->grid_blocks, blk, 0, s>>>(a);
+        } else {
+            if (fwd) batch_kernel<true, false><<<b->grid_blocks, blk, 0, s>>>(a);
+            else batch_kernel<false, false><<<b->grid_blocks, blk, 0, s>>>(a);
+        }
         NEFCT_CHECK_LAUNCH("batch_kernel (cubic voxels)");
     }
     if (b->split < total) {
         a.begin = b->split; a.end = total; a.counter = counter + 1;
-        if (fwd) batch_kernel<true, true><<<b->grid_blocks, blk, 0, s>>>(a);
-        else batch_kernel<false, true><<<b->grid_blocks, blk, 0, s>>>(a);
+        if (b->colwarp) {
+            if (fwd) batch_colwarp_kernel<true, true><<<b->grid_blocks, blk, 0, s>>>(a);
+            else batch_colwarp_kernel<false, true><<<b->grid_blocks, blk, 0, s>>>(a);
+        } else {
+            if (fwd) batch_kernel<true, true><<<b->grid_blocks, blk, 0, s>>>(a);
+            else batch_kernel<false, true><<<b->grid_blocks, blk, 0, s>>>(a);
+        }
         NEFCT_CHECK_LAUNCH("batch_kernel (other voxels)");
     }
     if (!fwd) {
         for (int i = 0; i < n; ++i) {
             const BatchDesc &D = b->desc[i];
+            if (b->colwarp) {
+                nefct_status st = zfold(D.volT, D.back, b->probs[b->order[i]].geom.grid, s);
+                if (st) return st;
+                continue;
+            }
             dim3 tg((D.g.nx + 31) / 32, (D.g.ny + 31) / 32, D.g.nz);
             fold_add_kernel<float><<<tg, dim3(32, 8), 0, s>>>(D.volT, D.back, D.g.nx, D.g.ny);
             NEFCT_CHECK_LAUNCH("fold_add_kernel (batch)");
@@ -248,6 +312,10 @@ nefct_status nefct_cb_batch_plan(const nefct_cb_problem *problems, int32_t n, ui
     }
     b->flags = flags;
     b->rows = tune_get(NEFCT_TUNE_CB_ROWS);
+    b->colwarp = tune_get(NEFCT_TUNE_CB_WALK) == 3;
+    for (int i = 0; i < n; ++i)
+        b->colwarp = b->colwarp && cb_use_colwarp<float>(problems[i].geom.grid, flags, true) &&
+                     cb_use_colwarp<float>(problems[i].geom.grid, flags, false);
     // cubic-voxel problems first (one kernel variant each), longest rays
     // first within each group: a tile's cost grows with its rays' slab count
     auto cubic = [&](int i) {
@@ -273,8 +341,8 @@ nefct_status nefct_cb_batch_plan(const nefct_cb_problem *problems, int32_t n, ui
         D.g = make_grid_dev<float>(g.grid);
         D.rg = make_ray_geom<float>(g);
         D.na = g.na; D.nb = g.nb; D.nv = g.nv;
-        D.tiles_a = (g.na + 31) / 32;
-        D.tiles_b = (g.nb + b->rows - 1) / b->rows;
+        D.tiles_a = b->colwarp ? (g.na + b->rows - 1) / b->rows : (g.na + 31) / 32;
+        D.tiles_b = b->colwarp ? (g.nb + 31) / 32 : (g.nb + b->rows - 1) / b->rows;
         D.cubic = D.g.dy == 1.f && D.g.dz == 1.f;
         D.flags = flags;
         b->t0[k + 1] = b->t0[k] + (long long)D.tiles_a * D.tiles_b * g.nv;
@@ -333,8 +401,12 @@ nefct_status nefct_cb_batch_bind(nefct_cb_batch *b, void *workspace, size_t byte
     NEFCT_CHECK_CUDA(cudaGetDevice(&dev));
     NEFCT_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     int lo = 1 << 30;
-    for (const void *k : {(const void *)batch_kernel<true, false>, (const void *)batch_kernel<true, true>,
-                          (const void *)batch_kernel<false, false>, (const void *)batch_kernel<false, true>}) {
+    const void *kernels[4] = {(const void *)batch_kernel<true, false>, (const void *)batch_kernel<true, true>,
+                              (const void *)batch_kernel<false, false>, (const void *)batch_kernel<false, true>};
+    const void *colwarp_kernels[4] = {
+        (const void *)batch_colwarp_kernel<true, false>, (const void *)batch_colwarp_kernel<true, true>,
+        (const void *)batch_colwarp_kernel<false, false>, (const void *)batch_colwarp_kernel<false, true>};
+    for (const void *k : b->colwarp ? colwarp_kernels : kernels) {
         NEFCT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * b->rows, 0));
         lo = std::min(lo, per_sm);
     }

@@ -91,11 +91,63 @@ __global__ void __launch_bounds__(256) cb_backward_kernel(const __grid_constant_
     ray_backward<T, DIV, EXACT>(p.g, r, p.flags, y, p.out, p.outT);
 }
 
-// Column warps: warp = rows [32*tile, 32*tile + 32) of column ia at view iv.
-// FWD: gathers from the z-fastest copy p.volT into the sinogram p.out;
-// otherwise reduces into the z-fastest accumulator p.outT.  Rays without a
-// contribution (outside the detector, missing the grid, zero value) stay in
-// the warp's walk with every slot inactive.
+// One lane of a column warp (the whole warp calls it together).  has: the
+// lane has a ray r; FWD: gathers from the z-fastest copy volZ into *out;
+// otherwise reduces y times the ray's weights into the z-fastest accumulator
+// accZ.  Rays without a contribution (outside the detector, missing the
+// grid, zero value) stay in the warp's walk with every slot inactive.
+template <bool DIV, bool FWD>
+__device__ __forceinline__ void colwarp_lane(const GridDev<float> &g, const float *r, bool has, uint32_t flags,
+                                             const float *__restrict__ volZ, float *out, float y, float *accZ)
+{
+    Walk<float> w{};
+    const bool live = has && (FWD || y != 0.f) && setup_walk(g, r, flags, w);
+    if (!__any_sync(0xffffffffu, live)) {
+        if (FWD && has) *out = 0.f;
+        return;
+    }
+    ColShared c;
+    ColLane L;
+    int K0, K1, KI0, KI1;
+    if (!col_setup(g, w, live, c, L, K0, K1, KI0, KI1)) {
+        // rays of the column disagree on the shared parameters: walk alone
+        unsigned su, sv;
+        col_strides(g, w.xdrive, su, sv);
+        if (FWD) {
+            const float v = live ? gather_walk<float, DIV, false, false>(w, g, volZ, (int)su, (int)sv, 1) : 0.f;
+            if (has) *out = v;
+        } else if (live) {
+            scatter_walk<float, DIV, false, false>(w, g, accZ, (int)su, (int)sv, 1, y);
+        }
+        return;
+    }
+    if (FWD) {
+        float acc = 0.f;
+        // interior slabs load every slot unpredicated: an inactive slot has
+        // ratio 0 and a valid index (so a volume holding +-inf may give NaN
+        // where the reference gives +-inf); lanes without a ray are discarded
+        auto f = [&](const auto &s) {
+            float v[s.n];
+#pragma unroll
+            for (int i = 0; i < s.n; ++i) v[i] = (!s.checked || s.ok[i]) ? __ldg(volZ + s.idx[i]) : 0.f;
+#pragma unroll
+            for (int i = 0; i < s.n; ++i) acc += v[i] * s.r[i];
+        };
+        col_walk_any<DIV, false>(c, L, K0, K1, KI0, KI1, g, f);
+        if (has) *out = live ? acc * w.W : 0.f;
+    } else {
+        const float yw = y * w.W;
+        auto f = [&](const auto &s) {
+#pragma unroll
+            for (int i = 0; i < s.n; ++i)
+                if (s.ok[i]) atomicAdd(accZ + s.idx[i], yw * s.r[i]);
+        };
+        col_walk_any<DIV, true>(c, L, K0, K1, KI0, KI1, g, f);
+    }
+}
+
+// Column warps: warp = rows [32*tile, 32*tile + 32) of column ia at view iv,
+// over the z-fastest copy p.volT (forward, into p.out) or accumulator p.outT.
 template <bool DIV, bool FWD>
 __global__ void __launch_bounds__(256) cb_colwarp_kernel(const __grid_constant__ CBParams<float> p)
 {
@@ -110,53 +162,8 @@ __global__ void __launch_bounds__(256) cb_colwarp_kernel(const __grid_constant__
     if (!FWD && has) y = cb_sino_value(p, ia, ib, iv);
     float r[6];
     cb_ray(p, ia, has ? ib : 0, iv, r);
-    Walk<float> w{};
-    const bool live = has && (FWD || y != 0.f) && setup_walk(p.g, r, p.flags, w);
-    float *const sino_out = FWD ? p.out + (size_t)(p.v0 + iv) * p.na * p.nb + (size_t)ib * p.na + ia : nullptr;
-    if (!__any_sync(0xffffffffu, live)) {
-        if (FWD && has) *sino_out = 0.f;
-        return;
-    }
-    ColShared c;
-    ColLane L;
-    int K0, K1, KI0, KI1;
-    if (!col_setup(p.g, w, live, c, L, K0, K1, KI0, KI1)) {
-        // rays of the column disagree on the shared parameters: walk alone
-        unsigned su, sv;
-        col_strides(p.g, w.xdrive, su, sv);
-        if (FWD) {
-            const float v = live ? gather_walk<float, DIV, false, false>(w, p.g, p.volT, (int)su, (int)sv, 1) : 0.f;
-            if (has) *sino_out = v;
-        } else if (live) {
-            scatter_walk<float, DIV, false, false>(w, p.g, p.outT, (int)su, (int)sv, 1, y);
-        }
-        return;
-    }
-    if (FWD) {
-        const float *__restrict__ src = p.volT;
-        float acc = 0.f;
-        // interior slabs load every slot unpredicated: an inactive slot has
-        // ratio 0 and a valid index (so a volume holding +-inf may give NaN
-        // where the reference gives +-inf); lanes without a ray are discarded
-        auto f = [&](const auto &s) {
-            float v[s.n];
-#pragma unroll
-            for (int i = 0; i < s.n; ++i) v[i] = (!s.checked || s.ok[i]) ? __ldg(src + s.idx[i]) : 0.f;
-#pragma unroll
-            for (int i = 0; i < s.n; ++i) acc += v[i] * s.r[i];
-        };
-        col_walk_any<DIV, false>(c, L, K0, K1, KI0, KI1, p.g, f);
-        if (has) *sino_out = live ? acc * w.W : 0.f;
-    } else {
-        float *dst = p.outT;
-        const float yw = y * w.W;
-        auto f = [&](const auto &s) {
-#pragma unroll
-            for (int i = 0; i < s.n; ++i)
-                if (s.ok[i]) atomicAdd(dst + s.idx[i], yw * s.r[i]);
-        };
-        col_walk_any<DIV, true>(c, L, K0, K1, KI0, KI1, p.g, f);
-    }
+    float *const out = FWD ? p.out + (size_t)(p.v0 + iv) * p.na * p.nb + (size_t)ib * p.na + ia : nullptr;
+    colwarp_lane<DIV, FWD>(p.g, r, has, p.flags, p.volT, out, y, p.outT);
 }
 
 // Launch shape of the thread walk for nvc views (see cb_cell).

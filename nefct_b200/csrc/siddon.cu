@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(256) zfold_kernel(const float *__restrict__ ac
 }
 
 // z-fastest copy [y][x][z] of an x-fastest volume (column-warp forward)
-static nefct_status zmajor_copy(const float *in, float *out, const nefct_grid &g, cudaStream_t s)
+nefct_status zmajor_copy(const float *in, float *out, const nefct_grid &g, cudaStream_t s)
 {
     dim3 grid((g.nx + 31) / 32, (g.nz + 31) / 32, g.ny);
     zmajor_kernel<<<grid, dim3(32, 8), 0, s>>>(in, out, g.nx, g.ny, g.nz);
@@ -261,7 +261,7 @@ static nefct_status zmajor_copy(const float *in, float *out, const nefct_grid &g
 }
 
 // vol = the x-fastest layout of the z-fastest accumulator (column-warp transpose)
-static nefct_status zfold(const float *acc, float *vol, const nefct_grid &g, cudaStream_t s)
+nefct_status zfold(const float *acc, float *vol, const nefct_grid &g, cudaStream_t s)
 {
     dim3 grid((g.nx + 31) / 32, (g.nz + 31) / 32, g.ny);
     zfold_kernel<<<grid, dim3(32, 8), 0, s>>>(acc, vol, g.nx, g.ny, g.nz);
@@ -278,11 +278,12 @@ static nefct_status transpose_xy(const T *in, T *out, const nefct_grid &g, cudaS
     return NEFCT_OK;
 }
 
-// Launches of the forward / transpose kernels for one problem whose
-// y-fastest volume copy (forward) or accumulator (transpose) is given; no
-// transpose, memset or fold.  Used by the batch's per-problem strategy.
+// Launches of the forward / transpose kernels for one problem whose volume
+// copy (forward) or accumulator (transpose) is given -- y-fastest for the
+// thread walk, z-fastest for column warps (colwarp); no transpose, memset or
+// fold.  Used by the batch's per-problem strategy.
 nefct_status cb_forward_launches(const nefct_cb_geom *g, const float *vol, const float *volT, float *sino,
-                                 uint32_t flags, cudaStream_t s)
+                                 uint32_t flags, cudaStream_t s, bool colwarp)
 {
     CBParams<float> p;
     fill_cb_params(p, g, flags);
@@ -292,14 +293,14 @@ nefct_status cb_forward_launches(const nefct_cb_geom *g, const float *vol, const
     for (int v0 = 0; v0 < g->nv; v0 += ViewTable<float>::kMax) {
         const int nvc = std::min(ViewTable<float>::kMax, g->nv - v0);
         fill_views(p, g, v0, nvc);
-        const cudaError_t e = cb_launch_forward<float>(p, g->na, g->nb, nvc, flags, s);
+        const cudaError_t e = cb_launch_forward<float>(p, g->na, g->nb, nvc, flags, s, colwarp);
         if (e != cudaSuccess) return cuda_fail(e, "cb_forward_kernel");
     }
     return NEFCT_OK;
 }
 
 nefct_status cb_backward_launches(const nefct_cb_geom *g, const float *sino, float *out, float *outT,
-                                  uint32_t flags, cudaStream_t s)
+                                  uint32_t flags, cudaStream_t s, bool colwarp)
 {
     CBParams<float> p;
     fill_cb_params(p, g, flags);
@@ -309,7 +310,7 @@ nefct_status cb_backward_launches(const nefct_cb_geom *g, const float *sino, flo
     for (int v0 = 0; v0 < g->nv; v0 += ViewTable<float>::kMax) {
         const int nvc = std::min(ViewTable<float>::kMax, g->nv - v0);
         fill_views(p, g, v0, nvc);
-        const cudaError_t e = cb_launch_backward<float>(p, g->na, g->nb, nvc, flags, s);
+        const cudaError_t e = cb_launch_backward<float>(p, g->na, g->nb, nvc, flags, s, colwarp);
         if (e != cudaSuccess) return cuda_fail(e, "cb_backward_kernel");
     }
     return NEFCT_OK;

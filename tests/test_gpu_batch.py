@@ -12,16 +12,21 @@ from tests.test_gpu_siddon import assert_parity
 pytestmark = pytest.mark.gpu
 
 
-def _thread_walk_forward(v, g, flags=0):
-    """Per-problem forward with the thread-per-ray walk, the per-ray code the
-    batch kernels share (bitwise comparable)."""
-    from nefct_b200 import autotune
-    saved = autotune.current()
-    try:
-        autotune.apply(saved["rows"], saved["order"], 0)
-        return ops.cb_forward(v, g, flags)
-    finally:
-        autotune.apply(saved["rows"], saved["order"], saved["walk"])
+class _walk:
+    """Context: the walk of both directions (0 thread per ray, 3 column
+    warps); a batch plan fixes its walk when it is made."""
+
+    def __init__(self, walk):
+        self.walk = walk
+
+    def __enter__(self):
+        from nefct_b200 import autotune
+        self.saved = autotune.current()
+        autotune.apply(self.saved["rows"], self.saved["order"], self.walk)
+
+    def __exit__(self, *exc):
+        from nefct_b200 import autotune
+        autotune.apply(self.saved["rows"], self.saved["order"], self.saved["walk"])
 
 
 def _problems(dev):
@@ -43,35 +48,39 @@ def _problems(dev):
     return geoms, vols, grads
 
 
+@pytest.mark.parametrize("walk", [0, 3], ids=["thread-walk", "column-warps"])
 @pytest.mark.parametrize("strategy", ["persistent", "per-problem"])
 @pytest.mark.parametrize("flags", [0, nb._lib.LINE_INTEGRAL])
-def test_batch_matches_per_problem(cuda, flags, strategy):
+def test_batch_matches_per_problem(cuda, flags, strategy, walk):
     geoms, vols, grads = _problems(cuda)
-    bp = BatchProjector(geoms, vols, grads=grads, flags=flags, strategy=strategy)
-    bp.step()
-    torch.cuda.synchronize()
-    for g, v, gr, s, b in zip(geoms, vols, grads, bp.sinos, bp.backs):
-        ref = _thread_walk_forward(v, g, flags)
-        assert torch.equal(s, ref)                       # same per-ray code: bitwise
-        assert_parity(b.cpu().numpy(), ops.cb_backward(gr, g, flags).cpu().numpy())
+    with _walk(walk):
+        bp = BatchProjector(geoms, vols, grads=grads, flags=flags, strategy=strategy)
+        bp.step()
+        torch.cuda.synchronize()
+        for g, v, gr, s, b in zip(geoms, vols, grads, bp.sinos, bp.backs):
+            ref = ops.cb_forward(v, g, flags)
+            assert torch.equal(s, ref)                   # same per-ray code: bitwise
+            assert_parity(b.cpu().numpy(), ops.cb_backward(gr, g, flags).cpu().numpy())
 
 
+@pytest.mark.parametrize("walk", [0, 3], ids=["thread-walk", "column-warps"])
 @pytest.mark.parametrize("strategy", ["persistent", "per-problem"])
-def test_batch_graph_replay(cuda, strategy):
+def test_batch_graph_replay(cuda, strategy, walk):
     geoms, vols, grads = _problems(cuda)
-    bp = BatchProjector(geoms, vols, grads=grads, strategy=strategy)
-    graph = bp.capture()
-    for b in bp.backs:
-        b.zero_()
-    for s in bp.sinos:
-        s.fill_(float("nan"))
-    graph.replay()
-    graph.replay()
-    torch.cuda.synchronize()
-    for g, v, gr, s, b in zip(geoms, vols, grads, bp.sinos, bp.backs):
-        assert torch.equal(s, _thread_walk_forward(v, g))
-        assert_parity(b.cpu().numpy(), ops.cb_backward(gr, g).cpu().numpy())
-    assert bp.tiles > 0
+    with _walk(walk):
+        bp = BatchProjector(geoms, vols, grads=grads, strategy=strategy)
+        graph = bp.capture()
+        for b in bp.backs:
+            b.zero_()
+        for s in bp.sinos:
+            s.fill_(float("nan"))
+        graph.replay()
+        graph.replay()
+        torch.cuda.synchronize()
+        for g, v, gr, s, b in zip(geoms, vols, grads, bp.sinos, bp.backs):
+            assert torch.equal(s, ops.cb_forward(v, g))
+            assert_parity(b.cpu().numpy(), ops.cb_backward(gr, g).cpu().numpy())
+        assert bp.tiles > 0
 
 
 def test_batch_auto_strategy_times_both(cuda):

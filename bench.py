@@ -1,6 +1,6 @@
 """Benchmark: cone-beam forward projection + exact adjoint on one B200.
 
-Workload (default, the FDK configuration's scanner): 256^3 float32 volume of
+Workload (default, the FDK scanner): 256^3 float32 volume of
 1 mm voxels holding 30 seeded ellipsoids, 360 views over 360 deg, flat
 detector 512 x 384 at 1.2 mm, source-axis 600 mm, source-detector 1200 mm.
 One step = forward projection (reference slab-split weights) of the volume
@@ -310,7 +310,7 @@ def run_gpu(args):
                                                                    else "thread per ray"},
                                                           "autotune_ms": tuned["ms"]}}
 
-    # FDK of this scanner (configuration 2): line-integral projections of the
+    # FDK of this scanner (256^3, 360 views): line-integral projections of the
     # phantom, cosine weight + ramp filter + weighted voxel-driven backprojection
     from nefct_b200 import recon
     fdk = {}
@@ -370,9 +370,9 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
-# ---------------- batched uneven problems (configuration 4) ----------------
+# ---------------- batched uneven problems (64 problems, edges 64..384) ----------------
 
-def config4_geoms(n_problems=64, seed=4, scale=1.0):
+def uneven_geoms(n_problems=64, seed=4, scale=1.0):
     """Seeded uneven problems: edge log-uniform in [64, 384] (times scale),
     views U{60..720}, detector rows/cols U{128..1024} (times scale), source-axis
     U[400, 700] mm, source-detector = source-axis x U[1.5, 2.0], 1 mm voxels,
@@ -402,7 +402,7 @@ def run_batched(args):
     from nefct_b200.batch import BatchProjector
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    geoms = config4_geoms(args.problems, 4, args.scale)
+    geoms = uneven_geoms(args.problems, 4, args.scale)
     gen = torch.Generator(device=dev).manual_seed(4)
     vols = [torch.rand(g.vol_shape, device=dev, generator=gen) for g in geoms]
     bp = BatchProjector(geoms, vols)            # grads = the forward outputs (loss = |Ax|^2 / 2)
@@ -460,7 +460,7 @@ def run_batched(args):
     print(json.dumps(line), flush=True)
 
 
-# ---------------- differentiable projector at 512^3 (configuration 3) ----------------
+# ---------------- differentiable projector at 512^3, 720 views ----------------
 
 def run_diff512(args):
     """512^3 phantom (50 ellipsoids, seed 3), 720 views, 1024x768 at 1 mm,
@@ -515,7 +515,7 @@ def run_diff512(args):
     print(json.dumps(line), flush=True)
 
 
-# ---------------- motion-compensated 4D through the warp (configuration 5) ----------------
+# ---------------- motion-compensated 4D through the warp (10 phases x 72 views) ----------------
 
 def run_motion4d(args):
     """256^3 reference volume, 10 phases x 72 views, 512x384, per-phase
@@ -577,7 +577,7 @@ def main():
     ap.add_argument("--walk", type=int, default=3,
                     help="with --rows: column warps for the forward (bit 0) / adjoint (bit 1), else thread per ray")
     ap.add_argument("--workload", default="fdk-scanner", choices=["fdk-scanner", "batched", "diff512", "motion4d"],
-                    help="batched: the uneven-problems configuration (its own JSON line)")
+                    help="batched: the 64 uneven problems (its own JSON line)")
     ap.add_argument("--problems", type=int, default=64)
     ap.add_argument("--scale", type=float, default=1.0, help="batched: scale of volume edges and detector sizes")
     args = ap.parse_args()

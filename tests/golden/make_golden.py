@@ -64,14 +64,12 @@ def main() -> None:
     vol = rng.random((16, 20, 24), dtype=np.float32)
     vals = rng.random(n, dtype=np.float32)
     g = oracle.grid(grid, centre, size)
-    ref_out = np.full(n, np.float32(-7.0))   # sentinel: the reference leaves Q4 rays unwritten
     out["lor/lors"] = lors
     out["lor/vol"] = vol
     out["lor/vals"] = vals
     fwd = oracle.ref_lor_forward(g, vol, lors)
     out["lor/fwd"] = fwd
     out["lor/bp"] = oracle.ref_lor_backward(g, vals, lors)
-    del ref_out
     # pixel_3d voxel-driven backprojection
     grid, size = (24, 20, 16), (48.0, 40.0, 32.0)
     corner = (-24.0 + 0.5, -20.0 - 0.5, -16.0 + 0.25)

@@ -141,8 +141,8 @@ def test_many_views_chunked_and_offsets(cuda, oracle_lib):
     assert_parity(out, ref)
 
 
-def test_config1_full_size_vs_reference(cuda, oracle_lib):
-    """Configuration 1 (64^3 at 2 mm, 10 seeded ellipsoids, 90 views, 128x96
+def test_64cube_90views_full_size_vs_reference(cuda, oracle_lib):
+    """The 64^3 workload (64^3 at 2 mm, 10 seeded ellipsoids, 90 views, 128x96
     at 2 mm, source-axis 500 mm, source-detector 1000 mm): forward and
     reference backprojection element-wise against the reference build (or
     the restatement when the build is absent)."""
@@ -199,7 +199,7 @@ def test_rays_missing_volume_are_zero(cuda):
 
 
 def test_linearity_and_adjoint_config2_size(cuda):
-    """Size-independent properties at configuration 2's full size (256^3,
+    """Size-independent properties at the 256^3 / 360-view workload's full size (256^3,
     360 views, 512x384): linearity, and <Ax,y> = <x,A^T y> in float32."""
     ang = np.linspace(0, 2 * np.pi, 360, endpoint=False)
     g = nb.ConeBeam((256, 256, 256), ang, 600.0, 1200.0, 512, 1.2, 384, 1.2, size=(256.0,) * 3)

@@ -13,7 +13,8 @@
 // rules, Q9-Q11, times (src_iso/(src_iso + x'))^2 from
 // mat_codes/backprojection.m:12): one thread owns a column of kZ voxels
 // along z; per view it computes the column's rotated position, detector
-// column and magnification once and then the kZ row taps.  Views are
+// column and magnification once and then the kZ row taps (one fused
+// multiply-add, an exact floor and four gathers per voxel and view).  Views are
 // processed in chunks so a chunk's filtered projections stay in L2.
 #include <math.h>
 #include <algorithm>
@@ -110,81 +111,119 @@ struct FilterParams {
     float taps[2 * kMaxCols - 1];  // h[d + na - 1], scale folded in (kernel parameter space)
 };
 
-static constexpr int kFiltThreads = 128;   // each thread owns 4 consecutive outputs
+static constexpr int kFiltThreads = 128;   // each thread owns 4 consecutive outputs per group
+static constexpr int kFiltRows = 4;        // detector rows per CTA (the taps are staged once)
+
+// Shared-memory layout of the filter: taps h[d] for d in [-8, 2na + 8) at
+// hs[d + kHPad + off] (zero outside [0, 2na - 2]), off in 0..3 chosen so that
+// a thread's tap window starts on a 16-byte boundary; then the weighted row
+// x[0..na) with a zero tail to a multiple of 4.
+static constexpr int kHPad = 8;
+__host__ __device__ static inline int filt_h_floats(int na) { return (2 * na + 2 * kHPad + 4 + 3) & ~3; }
+static inline size_t filt_smem_bytes(int na) { return (size_t)(filt_h_floats(na) + ((na + 3) & ~3) + 4) * sizeof(float); }
 
 __global__ void __launch_bounds__(kFiltThreads) fdk_filter_kernel(const __grid_constant__ FilterParams p,
                                                                   const float *__restrict__ sino,
                                                                   float *__restrict__ out)
 {
-    extern __shared__ float sm[];
+    extern __shared__ __align__(16) float sm[];
     const int na = p.na;
-    float *h = sm;                         // 2*na - 1 taps (+ padding)
-    float *x = sm + 2 * na + 3;            // weighted row, zero padded on both sides
-    const int row = blockIdx.x, iv = blockIdx.y;
-    for (int i = threadIdx.x; i < 2 * na - 1; i += blockDim.x) h[i] = p.taps[i];
-    const double v = ((double)row + p.b_shift) * p.db - (double)p.nb * p.db / 2.0;
-    const float *src = sino + ((size_t)iv * p.nb + row) * na;
-    for (int j = threadIdx.x; j < na; j += blockDim.x) {
-        const double u = ((double)j + p.a_shift) * p.da - (double)na * p.da / 2.0;
-        // cosine weight, filtering.m:10
-        double w = p.src_det / sqrt(p.src_det * p.src_det + u * u + v * v);
-        if (p.parker) {
-            // ParkerWeight.m:5-25 (view i is 1-based there)
-            const double as = atan(u / p.src_det) / M_PI * 180.0;
-            const double f = p.fanang;
-            const double n180 = 180.0 / p.dang;
-            const double pw = ((n180 - p.nv) / 2.0 + (iv + 1)) / n180 * 180.0 + p.parker * as;
-            if (pw <= f / 2 && pw > -f / 2) {
-                const double s = fmax(sin(M_PI / 2 * (f / 2 + pw) / f), 0.0);
-                w *= s * s;
-            }
-            if (pw >= 180 - f / 2 && pw < 180 + f / 2) {
-                const double c = fmax(cos(M_PI / 2 * (f / 2 + pw - 180) / f), 0.0);
-                w *= c * c;
-            }
-            if (pw < -f / 2 || pw > 180 + f / 2) w = 0.0;
-        }
-        x[j] = (float)((double)src[j] * w);
+    const int off = (5 - na) & 3;                     // (na - 5 + off) % 4 == 0
+    const int hn = filt_h_floats(na);
+    float *hs = sm;
+    float *x = sm + hn;
+    const int na4 = (na + 3) & ~3;
+    for (int i = threadIdx.x; i < hn; i += blockDim.x) {
+        const int d = i - kHPad - off;
+        hs[i] = (d >= 0 && d <= 2 * na - 2) ? p.taps[d] : 0.f;
     }
-    __syncthreads();
-    float *dst = out + ((size_t)iv * p.nb + row) * na;
-    // out[i] = sum_j x[j] h[i - j + na - 1]; a thread owns i0..i0+3 and keeps a
-    // sliding window of the four taps it needs (one new tap per step)
-    for (int i0 = 4 * threadIdx.x; i0 < na; i0 += 4 * blockDim.x) {
-        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-        const int base = i0 + na - 1;     // h index of (i0, j=0)
-        // window holds h[base - j + 0..3]; index beyond 2na-2 only when i0+k >= na (masked at store)
-        float w0 = h[base], w1 = base + 1 < 2 * na - 1 ? h[base + 1] : 0.f;
-        float w2 = base + 2 < 2 * na - 1 ? h[base + 2] : 0.f, w3 = base + 3 < 2 * na - 1 ? h[base + 3] : 0.f;
-        for (int j = 0; j < na; ++j) {
-            const float xj = x[j];
-            a0 = fmaf(xj, w0, a0);
-            a1 = fmaf(xj, w1, a1);
-            a2 = fmaf(xj, w2, a2);
-            a3 = fmaf(xj, w3, a3);
-            w3 = w2; w2 = w1; w1 = w0;
-            w0 = base - j - 1 >= 0 ? h[base - j - 1] : 0.f;
+    const int iv = blockIdx.y;
+    for (int row = blockIdx.x * kFiltRows; row < min(p.nb, (blockIdx.x + 1) * kFiltRows); ++row) {
+        __syncthreads();                                  // taps staged / previous row consumed
+        const double v = ((double)row + p.b_shift) * p.db - (double)p.nb * p.db / 2.0;
+        const float *src = sino + ((size_t)iv * p.nb + row) * na;
+        for (int j = threadIdx.x; j < na4; j += blockDim.x) {
+            if (j >= na) { x[j] = 0.f; continue; }
+            const double u = ((double)j + p.a_shift) * p.da - (double)na * p.da / 2.0;
+            // cosine weight, filtering.m:10
+            double w = p.src_det / sqrt(p.src_det * p.src_det + u * u + v * v);
+            if (p.parker) {
+                // ParkerWeight.m:5-25 (view i is 1-based there)
+                const double as = atan(u / p.src_det) / M_PI * 180.0;
+                const double f = p.fanang;
+                const double n180 = 180.0 / p.dang;
+                const double pw = ((n180 - p.nv) / 2.0 + (iv + 1)) / n180 * 180.0 + p.parker * as;
+                if (pw <= f / 2 && pw > -f / 2) {
+                    const double s = fmax(sin(M_PI / 2 * (f / 2 + pw) / f), 0.0);
+                    w *= s * s;
+                }
+                if (pw >= 180 - f / 2 && pw < 180 + f / 2) {
+                    const double c = fmax(cos(M_PI / 2 * (f / 2 + pw - 180) / f), 0.0);
+                    w *= c * c;
+                }
+                if (pw < -f / 2 || pw > 180 + f / 2) w = 0.0;
+            }
+            x[j] = (float)((double)src[j] * w);
         }
-        if (i0 < na) dst[i0] = a0;
-        if (i0 + 1 < na) dst[i0 + 1] = a1;
-        if (i0 + 2 < na) dst[i0 + 2] = a2;
-        if (i0 + 3 < na) dst[i0 + 3] = a3;
+        __syncthreads();
+        float *dst = out + ((size_t)iv * p.nb + row) * na;
+        // out[i] = sum_j x[j] h[i - j + na - 1], j ascending for every i.  A
+        // thread owns i0..i0+3; per block of four j it needs the taps
+        // h[D-3..D+3] (D = i0 + na - 1 - j0), held in an 8-wide register
+        // window w[k] = h[D - 4 + k] that slides by four per block (one
+        // 16-byte load), with the four x[j] broadcast by one 16-byte load.
+        for (int i0 = 4 * threadIdx.x; i0 < na; i0 += 4 * blockDim.x) {
+            float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+            const float *hp = hs + kHPad + off + (i0 + na - 5);    // &h[D - 4] for j0 = 0 (16-byte aligned)
+            float4 lo = *reinterpret_cast<const float4 *>(hp);     // w0..w3
+            float4 hi = *reinterpret_cast<const float4 *>(hp + 4); // w4..w7
+            for (int j0 = 0; j0 < na4; j0 += 4) {
+                const float4 xv = *reinterpret_cast<const float4 *>(x + j0);
+                a0 = fmaf(xv.x, hi.x, a0); a0 = fmaf(xv.y, lo.w, a0); a0 = fmaf(xv.z, lo.z, a0); a0 = fmaf(xv.w, lo.y, a0);
+                a1 = fmaf(xv.x, hi.y, a1); a1 = fmaf(xv.y, hi.x, a1); a1 = fmaf(xv.z, lo.w, a1); a1 = fmaf(xv.w, lo.z, a1);
+                a2 = fmaf(xv.x, hi.z, a2); a2 = fmaf(xv.y, hi.y, a2); a2 = fmaf(xv.z, hi.x, a2); a2 = fmaf(xv.w, lo.w, a2);
+                a3 = fmaf(xv.x, hi.w, a3); a3 = fmaf(xv.y, hi.z, a3); a3 = fmaf(xv.z, hi.y, a3); a3 = fmaf(xv.w, hi.x, a3);
+                hp -= 4;
+                hi = lo;
+                lo = *reinterpret_cast<const float4 *>(hp);
+            }
+            if (i0 < na) dst[i0] = a0;
+            if (i0 + 1 < na) dst[i0 + 1] = a1;
+            if (i0 + 2 < na) dst[i0 + 2] = a2;
+            if (i0 + 3 < na) dst[i0 + 3] = a3;
+        }
     }
 }
 
 // ---------------- device: voxel-driven backprojection ----------------
 
-static constexpr int kZ = 8;          // voxels along z per thread
+#ifndef NEFCT_FDK_KZ
+#define NEFCT_FDK_KZ 4
+#endif
+static constexpr int kZ = NEFCT_FDK_KZ; // voxels along z per thread
 static constexpr int kViewChunk = 32; // views per launch (L2-resident chunk)
 
 struct BpParams {
     int nx, ny, nz, na, nb, nv0, nvc, first;
     float sx, sy, sz, corner_x, corner_y, corner_z;
     float src_iso, src_det, da, ai_p, db, bi_p;
+    float inv_da, inv_db, cb;         // 1/da, 1/db and nb/2 - bi_p - 0.5, rounded to float
     int cyl, weight;
     float cs[kViewChunk], sn[kViewChunk];
 };
 
+// Per view the column part (rotation, magnification m, detector column a,
+// its bilinear weights, the distance weight) follows the reference's
+// operations with its divisions replaced by one approximate reciprocal of
+// the source distance (a few ulp; every weight is continuous in it);
+// (double)(t - ai) - 0.5 rounded to float equals the float subtraction
+// t - ai - 0.5f exactly (the double difference is exact), so no FP64 is
+// needed.  Per voxel the detector row is b = (m/db) * z + (nb/2 -
+// bi - 0.5) by one fused multiply-add (the reference's (m*z)/db + nb/2 - bi
+// - 0.5 rounds four times; the two differ by a few ulp of b, which moves the
+// bilinear weights continuously), clamped to [-2, nb + 1] (a voxel at the
+// source plane has an infinite or NaN b) and floored exactly by the
+// magic-constant sum (floor(b) + 1.5*2^23 = round-down(b + 1.5*2^23)).
 __global__ void __launch_bounds__(128) fdk_bp_kernel(const __grid_constant__ BpParams p,
                                                      const float *__restrict__ sino, float *__restrict__ vol)
 {
@@ -205,36 +244,41 @@ __global__ void __launch_bounds__(128) fdk_bp_kernel(const __grid_constant__ BpP
         acc[k] = (!p.first && iz < p.nz) ? vol[iz * plane + col] : 0.f;
     }
     const float xs = -p.src_iso;
-    const float nah = (float)(p.na / 2), nbh = (float)(p.nb / 2);   // integer halves (Q9)
+    const float nah = (float)(p.na / 2);   // integer half (Q9)
+    const float bhi = (float)(p.nb + 1);
+    const unsigned nb1 = (unsigned)(p.nb - 1);
     for (int v = 0; v < p.nvc; ++v) {
         const float cphi = p.cs[v], sphi = p.sn[v];
         const float xc0 = xc * cphi + yc * sphi;
         const float yc0 = -xc * sphi + yc * cphi;
-        const float m = __fdiv_rn(p.src_det, xc0 - xs);     // SAD / (xc0 - xs)
+        // 1 / (xc0 - xs) = 1 / (src_iso + xc0): magnification and distance weight share it
+        const float inv = rcp_approx(xc0 - xs);
+        const float m = p.src_det * inv;                       // SAD / (xc0 - xs)
         float t;
-        if (p.cyl) t = __fdiv_rn(atan2f(yc0, xc0 + p.src_iso), p.da) + nah;
-        else t = __fdiv_rn(m * yc0, p.da) + nah;
-        const float a = (float)((double)(t - p.ai_p) - 0.5);
+        if (p.cyl) t = atan2f(yc0, xc0 + p.src_iso) * p.inv_da + nah;
+        else t = m * yc0 * p.inv_da + nah;
+        const float a = __fsub_rn(__fsub_rn(t, p.ai_p), 0.5f);
         const int ia = __float2int_rd(a);
         if (ia < 0 || ia + 1 >= p.na) continue;               // Q11
         const float wa2 = a - (float)ia, wa = 1.f - wa2;
         float u = 1.f;
         if (p.weight) {
-            const float r = __fdiv_rn(p.src_iso, p.src_iso + xc0);
+            const float r = p.src_iso * inv;
             u = r * r;
         }
+        const float bm = m * p.inv_db;
         const float *pv = sino + (size_t)v * p.na * p.nb + ia;
 #pragma unroll
         for (int k = 0; k < kZ; ++k) {
-            const float tb = __fdiv_rn(m * zc[k], p.db) + nbh;
-            const float b = (float)((double)(tb - p.bi_p) - 0.5);
-            const int ib = __float2int_rd(b);
-            if (ib < 0 || ib + 1 >= p.nb) continue;
-            const float wb2 = b - (float)ib, wb = 1.f - wb2;
+            const float b = fminf(fmaxf(fmaf(bm, zc[k], p.cb), -2.f), bhi);
+            const float mb = __fadd_rd(b, 12582912.0f);
+            const unsigned ib = (unsigned)(__float_as_int(mb) - 0x4B400000);
+            if (ib >= nb1) continue;                           // ib < 0 || ib + 1 >= nb
+            const float wb2 = b - __fsub_rn(mb, 12582912.0f), wb = 1.f - wb2;
             const float *q = pv + (size_t)ib * p.na;
-            const float s = __ldg(q) * wa * wb + __ldg(q + p.na) * wa * wb2 + __ldg(q + 1) * wa2 * wb +
-                            __ldg(q + p.na + 1) * wa2 * wb2;
-            acc[k] += s * u;
+            const float r0 = fmaf(__ldg(q + 1), wa2, __ldg(q) * wa);
+            const float r1 = fmaf(__ldg(q + p.na + 1), wa2, __ldg(q + p.na) * wa);
+            acc[k] = fmaf(fmaf(r1, wb2, r0 * wb), u, acc[k]);
         }
     }
 #pragma unroll
@@ -287,8 +331,8 @@ nefct_status nefct_fdk_filter(const nefct_cb_geom *g, const float *sino, float *
     std::vector<float> taps = ramp_taps(g->na, window, scale);
     std::copy(taps.begin(), taps.end(), p.taps);
     cudaStream_t s = (cudaStream_t)stream;
-    const size_t smem = (size_t)(3 * g->na + 3) * sizeof(float);
-    fdk_filter_kernel<<<dim3(g->nb, g->nv), kFiltThreads, smem, s>>>(p, sino, out);
+    const size_t smem = filt_smem_bytes(g->na);
+    fdk_filter_kernel<<<dim3((g->nb + kFiltRows - 1) / kFiltRows, g->nv), kFiltThreads, smem, s>>>(p, sino, out);
     delete pp;
     NEFCT_CHECK_LAUNCH("fdk_filter_kernel");
     return NEFCT_OK;
@@ -312,6 +356,9 @@ nefct_status nefct_fdk_backproject(const nefct_cb_geom *g, const float *filtered
     p->src_iso = g->src_iso; p->src_det = g->src_det;
     // pixel_3d's `ai` is the siddon_3d `ai` minus one half (Q9)
     p->da = g->da; p->ai_p = g->a_shift - 0.5f; p->db = g->db; p->bi_p = g->b_shift - 0.5f;
+    p->inv_da = (float)(1.0 / (double)g->da);
+    p->inv_db = (float)(1.0 / (double)g->db);
+    p->cb = (float)((double)(g->nb / 2) - (double)p->bi_p - 0.5);
     p->cyl = g->det_kind == NEFCT_DET_CYL;
     p->weight = !(flags & NEFCT_FDK_NO_WEIGHT);
     cudaStream_t s = (cudaStream_t)stream;

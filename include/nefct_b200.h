@@ -290,6 +290,37 @@ nefct_status nefct_warp_grad_dvf_f64(const double *img, const double *mx, const 
                                      const double *gout, int32_t nx, int32_t ny, int32_t nz,
                                      double *gmx, double *gmy, double *gmz, void *stream);
 
+
+/* ---- distance-driven FDK backprojection ----
+ * Replaces back_project_flat_fdk_gpu / back_project_cyli_fdk_gpu
+ * (nefct/cc/distance_3d/dist_3d_back_fdk.cu.cc:257-298, kernel :17-255), the
+ * detector-driven part of the dist_3d_mod library that the reference's
+ * Project3D/BackProject3D load.  Geometry in voxel units with the grid centred
+ * on the rotation axis, as there: source at distance src_iso from the axis
+ * (the reference's SAD), detector at src_det from the source (its SID); bin
+ * (ia, ib) sits at a = (ia + 0.5) * da + a_offset - na * da / 2 (radians for
+ * det_kind NEFCT_DET_CYL), b likewise; per-view z offsets shift source and
+ * detector (NULL = 0).  Each bin spreads value * (footprint overlap in the
+ * transverse and z axes) * |p2 - p1| / |driving component| * the FDK weight
+ * src_iso^2 / (src_iso + x cos + y sin)^2 over the voxels of every slab of
+ * its driving axis.  vol ([nz][ny][nx]) is overwritten (the reference adds
+ * into the caller's buffer).  Workspace: nefct_dd_workspace_bytes (one
+ * volume, a z-fastest accumulator). */
+typedef struct nefct_dd_geom {
+    int32_t nx, ny, nz, nv;
+    const float *angles;       /* host, nv */
+    const float *z_offsets;    /* host, nv, or NULL */
+    float src_iso, src_det;
+    int32_t na;
+    float da, a_offset;
+    int32_t nb;
+    float db, b_offset;
+    int32_t det_kind;
+} nefct_dd_geom;
+size_t nefct_dd_workspace_bytes(const nefct_dd_geom *g);
+nefct_status nefct_dd_backproject(const nefct_dd_geom *g, const float *proj, float *vol, void *ws, size_t ws_bytes,
+                                  void *stream);
+
 #ifdef __cplusplus
 }
 #endif

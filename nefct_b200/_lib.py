@@ -61,6 +61,15 @@ class CBGeom(C.Structure):
                 ("det_kind", C.c_int32)]
 
 
+class DDGeom(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("nv", C.c_int32),
+                ("angles", C.POINTER(C.c_float)), ("z_offsets", C.POINTER(C.c_float)),
+                ("src_iso", C.c_float), ("src_det", C.c_float),
+                ("na", C.c_int32), ("da", C.c_float), ("a_offset", C.c_float),
+                ("nb", C.c_int32), ("db", C.c_float), ("b_offset", C.c_float),
+                ("det_kind", C.c_int32)]
+
+
 class CBProblem(C.Structure):
     _fields_ = [("geom", CBGeom), ("vol", C.c_void_p), ("sino", C.c_void_p), ("grad", C.c_void_p),
                 ("back", C.c_void_p)]
@@ -100,6 +109,8 @@ _PROTOS = {
     "nefct_warp_forward_f64": (_i32, [_vp, _vp, _vp, _vp, _i32, _i32, _i32, _vp, _vp]),
     "nefct_warp_adjoint_f64": (_i32, [_vp, _vp, _vp, _vp, _i32, _i32, _i32, _vp, _vp]),
     "nefct_warp_grad_dvf_f64": (_i32, [_vp, _vp, _vp, _vp, _vp, _i32, _i32, _i32, _vp, _vp, _vp, _vp]),
+    "nefct_dd_workspace_bytes": (C.c_size_t, [C.POINTER(DDGeom)]),
+    "nefct_dd_backproject": (_i32, [C.POINTER(DDGeom), _vp, _vp, _vp, C.c_size_t, _vp]),
 }
 
 _lib: C.CDLL | None = None

@@ -11,7 +11,11 @@ and output shapes as the registered ops, including their quirks:
   Q10; ``ai`` counts from the pixel centre, Q9);
 * ``siddon``     cpp/siddon/siddon_gpu.cc:11-35 -- Projection,
   Backprojection (LOR pair);
-* ``deform``     cpp/deform/deform.cc:12-22 -- Deform.
+* ``deform``     cpp/deform/deform.cc:12-22 -- Deform;
+* ``distance_3d`` nefct/cc/distance_3d/dist_3d_back_fdk.cu.cc:257-298 --
+  back_project_flat_fdk_gpu / back_project_cyli_fdk_gpu (host entry points
+  of the distance-driven FDK backprojection; the reference registers no op
+  for them).  They add into the caller's ``image``, as there.
 
 Tensors are CUDA torch tensors.  ``grid``/``center``/``size`` may be
 sequences or tensors; the reference reads them back from the device with
@@ -29,7 +33,7 @@ import torch
 
 from . import _lib, ops
 
-__all__ = ["siddon_3d", "pixel_3d", "siddon", "deform"]
+__all__ = ["siddon_3d", "pixel_3d", "siddon", "deform", "distance_3d"]
 
 
 def _host3(v, cast):
@@ -121,3 +125,24 @@ pixel_3d = types.SimpleNamespace(back_project_flat=_pixel_backproject(False),
                                  back_project_cyli=_pixel_backproject(True))
 siddon = types.SimpleNamespace(projection=_projection, backprojection=_backprojection)
 deform = types.SimpleNamespace(deform=_deform)
+
+
+def _dd_backproject(cyl):
+    def op(pv_values, shape, offsets, angles, nv, SID, SAD, da, ai, na, db, bi, nb, image):
+        """pv_values [nv][nb][na]; shape (nx, ny, nz); SID = source-detector,
+        SAD = source-axis (this file's naming); image (nx, ny, nz) over
+        x-fastest memory is added to and returned."""
+        nx, ny, nz = _host3(shape, int)
+        ang = _angles(angles)[:int(nv)]
+        off = None if offsets is None else np.asarray(
+            offsets.detach().cpu().numpy() if isinstance(offsets, torch.Tensor) else offsets, np.float32)
+        pv = pv_values.reshape(int(nv), int(nb), int(na))
+        vol = ops.dd_backproject(pv, (nx, ny, nz), ang, float(SAD), float(SID), float(da), float(db), float(ai),
+                                 float(bi), "cyl" if cyl else "flat", off)
+        image += vol.reshape(image.shape)
+        return image
+    return op
+
+
+distance_3d = types.SimpleNamespace(back_project_flat_fdk_gpu=_dd_backproject(False),
+                                    back_project_cyli_fdk_gpu=_dd_backproject(True))

@@ -295,6 +295,39 @@ def warp_invert(mx, my, mz, iters: int = 30):
     return ix, iy, iz
 
 
+def dd_backproject(proj, shape, angles, src_iso: float, src_det: float, da: float, db: float,
+                   a_offset: float = 0.0, b_offset: float = 0.0, det_kind: str = "flat", z_offsets=None):
+    """Distance-driven FDK-weighted backprojection (back_project_{flat,cyli}_fdk_gpu,
+    nefct/cc/distance_3d/dist_3d_back_fdk.cu.cc:257-298).
+
+    proj: float32 CUDA tensor [nv][nb][na]; shape (nx, ny, nz); geometry in
+    voxel units with the grid centred on the axis; src_iso = source-axis
+    (the reference's SAD), src_det = source-detector (its SID); bin ia sits at
+    (ia + 0.5) * da + a_offset - na * da / 2.  Returns [nz][ny][nx]."""
+    if not proj.is_cuda:
+        raise NefctError(_lib.ERR_INVALID, "dd_backproject needs a CUDA tensor (there is no CPU path)")
+    if proj.dtype != torch.float32 or proj.dim() != 3:
+        raise NefctError(_lib.ERR_INVALID, "proj must be float32 [nv][nb][na]")
+    proj = proj.contiguous()
+    nv, nb, na = proj.shape
+    ang = np.ascontiguousarray(np.asarray(angles, np.float32).reshape(-1))
+    if ang.size != nv:
+        raise NefctError(_lib.ERR_INVALID, f"{ang.size} angles for {nv} views")
+    off = None if z_offsets is None else np.ascontiguousarray(np.asarray(z_offsets, np.float32).reshape(-1))
+    nx, ny, nz = (int(v) for v in shape)
+    g = _lib.DDGeom(nx, ny, nz, nv, ang.ctypes.data_as(C.POINTER(C.c_float)),
+                    off.ctypes.data_as(C.POINTER(C.c_float)) if off is not None else None,
+                    float(src_iso), float(src_det), na, float(da), float(a_offset), nb, float(db), float(b_offset),
+                    _lib.DET_CYL if det_kind == "cyl" else _lib.DET_FLAT)
+    wn = _lib.load().nefct_dd_workspace_bytes(C.byref(g))
+    ws = torch.empty(wn, dtype=torch.uint8, device=proj.device)
+    out = torch.empty((nz, ny, nx), dtype=torch.float32, device=proj.device)
+    with torch.cuda.device(proj.device):
+        _lib.call("nefct_dd_backproject", C.byref(g), proj.data_ptr(), out.data_ptr(), ws.data_ptr(), wn,
+                  _stream(proj))
+    return out
+
+
 # ---------------- autograd ----------------
 
 class _Project(torch.autograd.Function):

@@ -228,6 +228,24 @@ def warp_invert(mx, my, mz, iters=30):
     return out
 
 
+def dd_backproject(proj, angles, shape, SID, SAD, na, da, ai, nb, db, bi, *, cyl=False, off=None,
+                   use_cosf=True):
+    """Distance-driven FDK-weighted backprojection (dist_3d_back_fdk): voxel
+    units, grid centred on the axis, SID = source-detector, SAD =
+    source-axis; proj is [nv][nb][na]."""
+    L = lib()
+    nx, ny, nz = shape
+    nv = len(angles)
+    cs, sn = trig(angles, use_cosf)
+    o = np.zeros(nv, np.float32) if off is None else _f32(off)
+    out = np.zeros((nz, ny, nx), np.float32)
+    L.or_dd_backproject_f32(_p(_f32(proj)), _p(_f32(cs)), _p(_f32(sn)), _p(o), C.c_int(nv), C.c_float(SID),
+                            C.c_float(SAD), C.c_int(nx), C.c_int(ny), C.c_int(nz), C.c_int(na), C.c_float(da),
+                            C.c_float(ai), C.c_int(nb), C.c_float(db), C.c_float(bi), C.c_int(int(cyl)),
+                            C.c_int(int(use_cosf)), _p(out))
+    return out
+
+
 # ---------------- the reference itself, compiled for the host ----------------
 
 def ref_cb_forward(g: Grid, vol, angles, SID, SAD, na, da, ai, nb, db, bi, *, cyl=False, f64=False):
@@ -305,4 +323,18 @@ def ref_deform(img, mx, my, mz):
     out = np.zeros_like(img)
     R.ref_deform(_p(img), _p(_f32(mx)), _p(_f32(my)), _p(_f32(mz)), C.c_int(nx), C.c_int(ny),
                  C.c_int(nz), _p(out))
+    return out
+
+
+def ref_dd_backproject(proj, angles, shape, SID, SAD, na, da, ai, nb, db, bi, *, cyl=False, off=None):
+    """back_project_{flat,cyli}_fdk_gpu of dist_3d_back_fdk.cu.cc:257-298
+    (into a zeroed volume)."""
+    R = ref()
+    nx, ny, nz = shape
+    nv = len(angles)
+    o = np.zeros(nv, np.float32) if off is None else _f32(off)
+    out = np.zeros((nz, ny, nx), np.float32)
+    R.ref_dd_backproject(C.c_int(int(cyl)), _p(_f32(proj)), C.c_int(nx), C.c_int(ny), C.c_int(nz), _p(o),
+                         _p(_f32(angles)), C.c_int(nv), C.c_float(SID), C.c_float(SAD), C.c_float(da),
+                         C.c_float(ai), C.c_int(na), C.c_float(db), C.c_float(bi), C.c_int(nb), _p(out))
     return out

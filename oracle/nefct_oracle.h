@@ -90,6 +90,14 @@ void or_deform_f64(const double *img, const double *mx, const double *my, const 
 void or_warp_invert_f32(const float *mx, const float *my, const float *mz, int nx, int ny, int nz, int iters,
                         float *ix, float *iy, float *iz);
 
+/* Distance-driven FDK-weighted backprojection of
+ * nefct/cc/distance_3d/dist_3d_back_fdk.cu.cc:17-298 (voxel units, grid
+ * centred on the axis, SID = source-detector, SAD = source-axis); cs/sn are
+ * the per-view cos/sin (or_trig_f32), off the per-view z offsets. */
+void or_dd_backproject_f32(const float *proj, const float *cs, const float *sn, const float *off, int nv,
+                           float SID, float SAD, int nx, int ny, int nz, int na, float da, float ai, int nb,
+                           float db, float bi, int cyl, int use_cosf, float *img);
+
 #ifdef __cplusplus
 }
 #endif

@@ -10,6 +10,8 @@
 //   lor.inc           cpp/siddon/siddon_gpu.cu.cc:6-698       LOR project/backproject + kernels
 //   pixel3d.inc       nefct/cc/pixel_3d/pixel.cu.cc:6-146     voxel-driven backprojection
 //   deform.inc        cpp/deform/deform.cu.cc:6-46            DeformKernel
+//   dd_fdk.inc        nefct/cc/distance_3d/dist_3d_back_fdk.cu.cc:6-255
+//                                                             back_project_fdk_kernel (distance-driven)
 //
 // Kernels run as plain functions: a launch is emulated by setting the
 // thread-local blockIdx/threadIdx/blockDim/gridDim and calling the kernel
@@ -45,6 +47,14 @@ namespace dfm {
 #include "deform.inc"
 }
 #undef abs
+namespace ddf {
+#include "dd_fdk.inc"
+}
+#undef ABS
+#undef MAX
+#undef MIN
+#undef MAX4
+#undef MIN4
 
 // FP64 build of the siddon_3d walk: every float of the included ranges
 // becomes double, cosf/sinf become cos/sin.
@@ -251,6 +261,34 @@ void ref_deform(const float *img, const float *mx, const float *my, const float 
                 set_thread(gx, gy, gz, 16, 16, 4, ix, iy, iz);
                 dfm::DeformKernel(img, mx, my, mz, nx, ny, nz, img1);
             }
+}
+
+// back_project_flat_fdk_gpu / back_project_cyli_fdk_gpu of
+// dist_3d_back_fdk.cu.cc:257-298 into image (overwritten; the reference
+// accumulates into the caller's buffer).  SID = source-detector, SAD =
+// source-axis (python naming there); voxel units, grid centred on the axis.
+void ref_dd_backproject(int cyl, const float *pv, int nx, int ny, int nz, const float *offsets,
+                        const float *angles, int nv, float SID, float SAD, float da, float ai, int na, float db,
+                        float bi, int nb, float *image)
+{
+    const unsigned gx = (na + 15) / 16, gy = (nb + 15) / 16, gz = (nv + 3) / 4;
+    const long long nvox = (long long)nx * ny * nz;
+    const int nth = omp_get_max_threads();
+    float *priv = (float *)calloc((size_t)nth * nvox, sizeof(float));
+#pragma omp parallel
+    {
+        float *mine = priv + (long long)omp_get_thread_num() * nvox;
+#pragma omp for schedule(static)
+        for (int iv = 0; iv < nv; ++iv)
+            for (int ib = 0; ib < nb; ++ib)
+                for (int ia = 0; ia < na; ++ia) {
+                    set_thread(gx, gy, gz, 16, 16, 4, ia, ib, iv);
+                    ddf::back_project_fdk_kernel(cyl, angles, offsets, nv, SID, SAD, nx, ny, nz, da, ai, na, db,
+                                                 bi, nb, pv, mine);
+                }
+    }
+    sum_private(priv, nth, nvox, image);
+    free(priv);
 }
 
 }  // extern "C"

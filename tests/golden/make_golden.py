@@ -27,6 +27,12 @@ CASES = [
     ("cyl_iso", (24, 20, 16), (0.5, 0.5, -1.0), (48.0, 40.0, 32.0), True, 0.012),
 ]
 NV, NA, NB = 12, 40, 32
+# distance-driven case (voxel units; SID = source-detector, SAD = source-axis there)
+DD_GRID = (24, 20, 16)
+DD_SID, DD_SAD = 200.0, 100.0
+DD_NA, DD_DA, DD_DA_CYL, DD_AI = 40, 1.1, 0.011, 0.3
+DD_NB, DD_DB, DD_BI = 28, 1.2, -0.2
+DD_OFF = np.linspace(-1.5, 1.5, NV).astype(np.float32)
 SRC_ISO, SRC_DET = 200.0, 400.0
 AI, BI, DB = 0.5, 0.5, 2.0
 
@@ -86,6 +92,13 @@ def main() -> None:
     out["deform/img"] = img
     out["deform/mx"], out["deform/my"], out["deform/mz"] = m
     out["deform/out"] = oracle.ref_deform(img, *m)
+    # distance-driven FDK backprojection (dist_3d_back_fdk): voxel units
+    proj = rng.random((NV, DD_NB, DD_NA), dtype=np.float32)
+    out["dd/proj"] = proj
+    out["dd/off"] = DD_OFF
+    for key, cyl, da in (("dd/flat", False, DD_DA), ("dd/cyl", True, DD_DA_CYL)):
+        out[key] = oracle.ref_dd_backproject(proj, angles, DD_GRID, DD_SID, DD_SAD, DD_NA, da, DD_AI, DD_NB,
+                                             DD_DB, DD_BI, cyl=cyl, off=DD_OFF)
     np.savez_compressed(os.path.join(HERE, "golden.npz"), **out)
     print("wrote", os.path.join(HERE, "golden.npz"), sum(v.nbytes for v in out.values()), "bytes raw")
 

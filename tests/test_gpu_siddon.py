@@ -198,7 +198,7 @@ def test_rays_missing_volume_are_zero(cuda):
     assert float(out.abs().max()) == 0.0
 
 
-def test_linearity_and_adjoint_config2_size(cuda):
+def test_linearity_and_adjoint_256cube_360views(cuda):
     """Size-independent properties at the 256^3 / 360-view workload's full size (256^3,
     360 views, 512x384): linearity, and <Ax,y> = <x,A^T y> in float32."""
     ang = np.linspace(0, 2 * np.pi, 360, endpoint=False)
@@ -357,3 +357,46 @@ def test_exact_mode_adjoint_identity_f64(cuda, flags):
     lhs = float((ops.cb_forward(x, g, flags) * y).sum())
     rhs = float((x * ops.cb_backward(y, g, flags)).sum())
     assert abs(lhs - rhs) <= 1e-10 * abs(lhs)
+
+
+# Odd geometries for both walks against the restatement (same per-view trig):
+# steep cone (z slope > 1 per slab, z floors jump by 2), odd grid counts,
+# a single detector row / column, views on the axes and on the diagonal,
+# z offsets that push whole views out of the grid, a 1-voxel-thick grid.
+_EDGE = {
+    "steep_cone": dict(shape=(20, 20, 20), src_iso=25.0, src_det=50.0, na=24, da=2.0, nb=64, db=3.0),
+    "odd_counts": dict(shape=(33, 17, 9), src_iso=90.0, src_det=180.0, na=41, da=1.7, nb=23, db=1.3),
+    "one_row": dict(shape=(24, 24, 12), src_iso=80.0, src_det=160.0, na=50, da=1.0, nb=1, db=1.0),
+    "one_column": dict(shape=(24, 24, 12), src_iso=80.0, src_det=160.0, na=1, da=1.0, nb=40, db=0.8),
+    "thin_grid": dict(shape=(30, 28, 1), src_iso=70.0, src_det=140.0, na=36, da=1.5, nb=9, db=0.4),
+}
+_EDGE_ANGLES = np.array([0.0, np.pi / 4, np.pi / 2, 0.7, np.pi, 3 * np.pi / 4, 5.5], np.float32)
+
+
+@pytest.mark.parametrize("walk", [0, 3], ids=["thread-walk", "column-warps"])
+@pytest.mark.parametrize("name", sorted(_EDGE))
+def test_edge_geometries_vs_restatement(cuda, oracle_lib, name, walk):
+    from nefct_b200 import autotune
+    e = _EDGE[name]
+    off = np.array([0.0, 0.5, -0.5, 40.0, 0.0, -1.0, 0.25], np.float32)      # view 3 mostly misses the grid
+    g = nb.ConeBeam(e["shape"], _EDGE_ANGLES, e["src_iso"], e["src_det"], e["na"], e["da"], e["nb"], e["db"],
+                    size=tuple(float(v) for v in e["shape"]), z_offsets=off)
+    rng = np.random.default_rng(5)
+    vol = rng.random(g.vol_shape, dtype=np.float32)
+    y = rng.random(g.sino_shape, dtype=np.float32)
+    og = oracle_lib.grid(e["shape"], (0, 0, 0), tuple(float(v) for v in e["shape"]))
+    args = (_EDGE_ANGLES, e["src_iso"], e["src_det"], e["na"], e["da"], 0.5, e["nb"], e["db"], 0.5)
+    ref_f, _ = oracle_lib.cb_forward(og, vol, *args, off=off)
+    ref_b = oracle_lib.cb_backward(og, y, *args, off=off, flags=oracle_lib.CB_FWD)
+    saved = autotune.current()
+    try:
+        autotune.apply(saved["rows"], saved["order"], walk)
+        out_f = ops.cb_forward(torch.from_numpy(vol).to(cuda), g).cpu().numpy()
+        out_b = ops.cb_backward(torch.from_numpy(y).to(cuda), g).cpu().numpy()
+    finally:
+        autotune.apply(saved["rows"], saved["order"], saved["walk"])
+    assert np.abs(ref_f).max() > 0
+    assert_parity(out_f, ref_f, rel=1e-6, mabs=1e-5)
+    assert_parity(out_b, ref_b, rel=1e-6, mabs=1e-5)
+    miss = ref_f == 0                      # rays that miss the grid (the volume has no zero voxel)
+    assert miss.any() and float(np.abs(out_f[miss]).max()) == 0.0

@@ -594,6 +594,122 @@ def run_motion4d(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------- per-row timings of the other operators on this path ----------------
+
+def run_rows(args):
+    """Device time of each operator beside the headline pair, on workloads of
+    the bench's sizes, with the reference's host build timed on a sample where
+    it has the operator: the LOR pair (16 Mi random PET-like lines through
+    256^3), the reference backprojection (Q8 off), the deterministic and the
+    exact-mode transposes and the exact-mode forward (36 views of the bench
+    scanner), the warp family at 256^3, and the distance-driven FDK
+    backprojection (72 views of the bench scanner in voxel units)."""
+    import torch
+    import nefct_b200 as nb
+    from nefct_b200 import _lib, ops
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    gen = torch.Generator(device=dev).manual_seed(9)
+    n = CFG["n"]
+
+    def timed(fn, reps=None):
+        reps = reps or max(1, args.steps)
+        for _ in range(max(1, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / reps
+
+    rows = {}
+    vol = torch.rand((n, n, n), device=dev, generator=gen)
+    # LOR pair: end points on a 300 mm ring (random angles, z in +-100 mm)
+    nl = 16 * 2 ** 20
+    rng = np.random.default_rng(9)
+    phi1, phi2 = rng.uniform(0, 2 * np.pi, nl), rng.uniform(0, 2 * np.pi, nl)
+    lors = np.stack([300 * np.cos(phi1), 300 * np.sin(phi1), rng.uniform(-100, 100, nl),
+                     300 * np.cos(phi2), 300 * np.sin(phi2), rng.uniform(-100, 100, nl)]).astype(np.float32)
+    d_lors = torch.from_numpy(lors).to(dev)
+    vals = torch.rand(nl, device=dev, generator=gen)
+    t_lf = timed(lambda: ops.lor_forward(d_lors, vol, (n, n, n)))
+    t_lb = timed(lambda: ops.lor_backward(d_lors, vals, (n, n, n)))
+    rows["lor_pair"] = {"lors": nl, "grid": [n] * 3, "forward_ms": 1e3 * t_lf, "backward_ms": 1e3 * t_lb,
+                        "forward_lors_per_s": nl / t_lf, "backward_lors_per_s": nl / t_lb}
+    # reference backprojection / deterministic / exact on 36 views of the bench scanner
+    ang = angles()[::10]
+    g = nb.ConeBeam((n, n, n), ang, CFG["src_iso"], CFG["src_det"], CFG["na"], CFG["pixel"], CFG["nb"],
+                    CFG["pixel"], size=(n * CFG["voxel"],) * 3)
+    y = torch.rand(g.sino_shape, device=dev, generator=gen)
+    back = torch.empty_like(vol)
+    i_fwd = ops.cb_count_intersections(g, 0, dev)
+    i_ref = ops.cb_count_intersections(g, _lib.REF_BACKPROJECT, dev)
+    t_atomic = timed(lambda: ops.cb_backward(y, g, 0, out=back))
+    t_refbp = timed(lambda: ops.cb_backward(y, g, _lib.REF_BACKPROJECT, out=back))
+    t_det = timed(lambda: ops.cb_backward(y, g, _lib.DETERMINISTIC, out=back))
+    sino = torch.empty(g.sino_shape, device=dev)
+    t_exf = timed(lambda: ops.cb_forward(vol, g, _lib.EXACT, out=sino))
+    t_exb = timed(lambda: ops.cb_backward(y, g, _lib.EXACT, out=back))
+    rows["cone_beam_36_views"] = {
+        "intersections_forward_walk": i_fwd, "intersections_reference_backprojection": i_ref,
+        "transpose_ms": 1e3 * t_atomic, "reference_backprojection_ms": 1e3 * t_refbp,
+        "reference_backprojection_intersections_per_s": i_ref / t_refbp,
+        "deterministic_transpose_ms": 1e3 * t_det, "deterministic_over_atomic": t_det / t_atomic,
+        "exact_mode_forward_ms": 1e3 * t_exf, "exact_mode_transpose_ms": 1e3 * t_exb}
+    # warp family at 256^3 (fields up to 5 voxels)
+    from nefct_b200 import recon
+    m = recon.sinusoid_field(vol.shape, 5.0, np.random.default_rng(5), device=dev)
+    gout = torch.rand_like(vol)
+    t_wf = timed(lambda: ops.warp_forward(vol, *m))
+    t_wa = timed(lambda: ops.warp_adjoint(gout, *m))
+    t_wg = timed(lambda: ops.warp_grad_dvf(vol, *m, gout))
+    t_wi = timed(lambda: ops.warp_invert(*m), reps=2)
+    nvox = n ** 3
+    rows["warp_256cube"] = {"forward_ms": 1e3 * t_wf, "forward_gbs_of_48B_per_voxel": 48 * nvox / t_wf / 1e9,
+                            "adjoint_ms": 1e3 * t_wa, "dvf_gradient_ms": 1e3 * t_wg,
+                            "invert_30_passes_ms": 1e3 * t_wi}
+    # distance-driven FDK backprojection: the bench scanner in voxel units, 72 views
+    ang72 = angles()[::5]
+    proj = torch.rand((ang72.size, CFG["nb"], CFG["na"]), device=dev, generator=gen)
+    px = CFG["pixel"] / CFG["voxel"]
+    sad, sid = CFG["src_iso"] / CFG["voxel"], CFG["src_det"] / CFG["voxel"]
+    t_dd = timed(lambda: ops.dd_backproject(proj, (n, n, n), ang72, sad, sid, px, px), reps=2)
+    rows["distance_driven_72_views"] = {"ms": 1e3 * t_dd, "bins_per_s": proj.numel() / t_dd}
+    # the reference's host build on samples of the same operators
+    if not args.no_cpu:
+        import oracle
+        if oracle.have_ref():
+            og = oracle.grid((n, n, n), (0, 0, 0), (float(n),) * 3)
+            hv = vol.cpu().numpy()
+            k = 2 ** 17
+            t0 = time.perf_counter()
+            oracle.ref_lor_forward(og, hv, np.ascontiguousarray(lors[:, :k]))
+            t_cpu_lor = time.perf_counter() - t0
+            mh = [c.cpu().numpy() for c in m]
+            t0 = time.perf_counter()
+            oracle.ref_deform(hv, *mh)
+            t_cpu_warp = time.perf_counter() - t0
+            ph = proj[:2].cpu().numpy()
+            t0 = time.perf_counter()
+            oracle.ref_dd_backproject(ph, ang72[:2], (n, n, n), sid, sad, CFG["na"], px, 0.0, CFG["nb"], px, 0.0)
+            t_cpu_dd = (time.perf_counter() - t0) * ang72.size / 2
+            rows["reference_host_build"] = {
+                "cores": os.cpu_count(), "lor_forward_lors_per_s": k / t_cpu_lor,
+                "lor_forward_speedup": (nl / t_lf) / (k / t_cpu_lor),
+                "warp_forward_ms": 1e3 * t_cpu_warp, "warp_forward_speedup": t_cpu_warp / t_wf,
+                "distance_driven_72_views_ms_from_2_view_sample": 1e3 * t_cpu_dd,
+                "distance_driven_speedup": t_cpu_dd / t_dd}
+    line = {"metric": "LOR forward + backward lines/s (16 Mi lines, 256^3); other operators in extras",
+            "value": nl / (t_lf + t_lb), "unit": "lines/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * (t_lf + t_lb), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded uniform volumes, lines, sinograms and fields)",
+            "config": {"workload": "per-operator timings beside the 256^3 / 360-view pair"}, "extras": rows}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -606,7 +722,8 @@ def main():
     ap.add_argument("--order", type=int, default=1, help="with --rows: 0 row bands outermost, 1 views outermost")
     ap.add_argument("--walk", type=int, default=3,
                     help="with --rows: column warps for the forward (bit 0) / adjoint (bit 1), else thread per ray")
-    ap.add_argument("--workload", default="fdk-scanner", choices=["fdk-scanner", "batched", "diff512", "motion4d"],
+    ap.add_argument("--workload", default="fdk-scanner",
+                    choices=["fdk-scanner", "batched", "diff512", "motion4d", "rows"],
                     help="batched: the 64 uneven problems (its own JSON line)")
     ap.add_argument("--problems", type=int, default=64)
     ap.add_argument("--scale", type=float, default=1.0, help="batched: scale of volume edges and detector sizes")
@@ -620,6 +737,8 @@ def main():
         run_diff512(args)
     elif args.workload == "motion4d":
         run_motion4d(args)
+    elif args.workload == "rows":
+        run_rows(args)
     else:
         run_gpu(args)
 

@@ -635,10 +635,16 @@ def run_rows(args):
                      300 * np.cos(phi2), 300 * np.sin(phi2), rng.uniform(-100, 100, nl)]).astype(np.float32)
     d_lors = torch.from_numpy(lors).to(dev)
     vals = torch.rand(nl, device=dev, generator=gen)
-    t_lf = timed(lambda: ops.lor_forward(d_lors, vol, (n, n, n)))
-    t_lb = timed(lambda: ops.lor_backward(d_lors, vals, (n, n, n)))
+    t_lf0 = timed(lambda: ops.lor_forward(d_lors, vol, (n, n, n)))
+    t_lb0 = timed(lambda: ops.lor_backward(d_lors, vals, (n, n, n)))
+    t_ord = timed(lambda: ops.lor_order(d_lors, (n, n, n)), reps=2)
+    order = ops.lor_order(d_lors, (n, n, n))
+    t_lf = timed(lambda: ops.lor_forward(d_lors, vol, (n, n, n), order=order))
+    t_lb = timed(lambda: ops.lor_backward(d_lors, vals, (n, n, n), order=order))
     rows["lor_pair"] = {"lors": nl, "grid": [n] * 3, "forward_ms": 1e3 * t_lf, "backward_ms": 1e3 * t_lb,
-                        "forward_lors_per_s": nl / t_lf, "backward_lors_per_s": nl / t_lb}
+                        "forward_lors_per_s": nl / t_lf, "backward_lors_per_s": nl / t_lb,
+                        "walk_order": "ordered (lor_order, computed once per list)", "order_ms": 1e3 * t_ord,
+                        "list_order_forward_ms": 1e3 * t_lf0, "list_order_backward_ms": 1e3 * t_lb0}
     # reference backprojection / deterministic / exact on 36 views of the bench scanner
     ang = angles()[::10]
     g = nb.ConeBeam((n, n, n), ang, CFG["src_iso"], CFG["src_det"], CFG["na"], CFG["pixel"], CFG["nb"],

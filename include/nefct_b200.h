@@ -231,6 +231,19 @@ nefct_status nefct_lor_forward(const nefct_grid *grid, const float *lors, int64_
                                float *out, uint32_t flags, void *stream);
 nefct_status nefct_lor_backward(const nefct_grid *grid, const float *lors, int64_t n, const float *vals,
                                 float *vol, uint32_t flags, void *stream);
+/* Walk order for large unsorted line lists (no counterpart in the reference,
+ * whose kernels walk lines in list order).  nefct_lor_order_keys writes a
+ * 31-bit key per line (driving axis, in-plane direction, distance from the
+ * grid centre, z, z slope); a permutation that sorts the keys (any stable or
+ * unstable sort) makes a warp's lines nearly parallel neighbours.  The
+ * *_ordered walks visit lines in that order and write each result at the
+ * line's own index: the same outputs as the unordered calls (the backward's
+ * atomic summation order differs).  Fewer than 2^31 lines. */
+nefct_status nefct_lor_order_keys(const nefct_grid *grid, const float *lors, int64_t n, int32_t *keys, void *stream);
+nefct_status nefct_lor_forward_ordered(const nefct_grid *grid, const float *lors, int64_t n, const int32_t *order,
+                                       const float *vol, float *out, uint32_t flags, void *stream);
+nefct_status nefct_lor_backward_ordered(const nefct_grid *grid, const float *lors, int64_t n, const int32_t *order,
+                                        const float *vals, float *vol, uint32_t flags, void *stream);
 
 /* FDK.  Filter windows of mat_codes/filtering.m:63-88. */
 #define NEFCT_WIN_RAM_LAK     0

@@ -100,6 +100,9 @@ _PROTOS = {
     "nefct_cb_batch_destroy": (None, [_vp]),
     "nefct_lor_forward": (_i32, [C.POINTER(Grid), _vp, C.c_int64, _vp, _vp, _u32, _vp]),
     "nefct_lor_backward": (_i32, [C.POINTER(Grid), _vp, C.c_int64, _vp, _vp, _u32, _vp]),
+    "nefct_lor_order_keys": (_i32, [C.POINTER(Grid), _vp, C.c_int64, _vp, _vp]),
+    "nefct_lor_forward_ordered": (_i32, [C.POINTER(Grid), _vp, C.c_int64, _vp, _vp, _vp, _u32, _vp]),
+    "nefct_lor_backward_ordered": (_i32, [C.POINTER(Grid), _vp, C.c_int64, _vp, _vp, _vp, _u32, _vp]),
     "nefct_fdk_filter": (_i32, [C.POINTER(CBGeom), _vp, _vp, _i32, _i32, _vp]),
     "nefct_fdk_backproject": (_i32, [C.POINTER(CBGeom), _vp, _vp, _u32, _vp]),
     "nefct_warp_forward": (_i32, [_vp, _vp, _vp, _vp, _i32, _i32, _i32, _vp, _vp]),

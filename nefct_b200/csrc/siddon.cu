@@ -113,13 +113,18 @@ template <typename T> struct LorParams {
     const T *vol;
     const T *vals;
     T *out;
+    const int32_t *order;     // walk order (a permutation of 0..n-1), or nullptr
 };
 
+// The walk visits lines in `order` so that a warp's 32 lines are nearly
+// parallel neighbours (similar trip counts, nearby voxels); results stay at
+// each line's own index.
 template <typename T, bool DIV, bool Q5>
 __global__ void __launch_bounds__(256) lor_forward_kernel(const __grid_constant__ LorParams<T> p)
 {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < p.n;
-         i += (long long)gridDim.x * blockDim.x) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < p.n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long i = p.order ? (long long)p.order[t] : t;
         T r[6];
         for (int j = 0; j < 6; ++j) r[j] = p.lors[j * p.n + i];
         Walk<T> w;
@@ -136,8 +141,9 @@ __global__ void __launch_bounds__(256) lor_forward_kernel(const __grid_constant_
 template <typename T, bool DIV, bool Q5>
 __global__ void __launch_bounds__(256) lor_backward_kernel(const __grid_constant__ LorParams<T> p)
 {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < p.n;
-         i += (long long)gridDim.x * blockDim.x) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < p.n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long i = p.order ? (long long)p.order[t] : t;
         const T y = p.vals[i];
         if (y == (T)0) continue;
         T r[6];
@@ -147,6 +153,40 @@ __global__ void __launch_bounds__(256) lor_backward_kernel(const __grid_constant
         const int sw = p.g.nx * p.g.ny;
         if (w.xdrive) scatter_walk<T, DIV, false, Q5>(w, p.g, p.out, 1, p.g.nx, sw, y);
         else scatter_walk<T, DIV, true, Q5>(w, p.g, p.out, p.g.nx, 1, sw, y);
+    }
+}
+
+// Ordering key of a line (31 bits, larger = later): driving axis, in-plane
+// direction folded to [0, pi), signed distance of the in-plane line from the
+// grid centre, z where the line passes the centre, and z slope.  Lines with
+// equal keys are nearly parallel neighbours.
+__global__ void __launch_bounds__(256) lor_key_kernel(const __grid_constant__ LorParams<float> p, int32_t *keys)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < p.n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const float x1 = p.lors[i] - p.g.cx, y1 = p.lors[p.n + i] - p.g.cy, z1 = p.lors[2 * p.n + i] - p.g.cz;
+        const float dx = p.lors[3 * p.n + i] - p.g.cx - x1, dy = p.lors[4 * p.n + i] - p.g.cy - y1;
+        const float dz = p.lors[5 * p.n + i] - p.g.cz - z1;
+        const float sx = (float)p.g.nx * p.g.dx_, sy = p.g.dy * (float)p.g.ny * p.g.dx_;
+        const float sz = p.g.dz * (float)p.g.nz * p.g.dx_;
+        const float lxy = sqrtf(dx * dx + dy * dy);
+        const unsigned xdrive = fabsf(dx) >= fabsf(dy);
+        float th = atan2f(dy, dx);
+        if (th < 0.f) th += 3.14159265f;
+        if (th >= 3.14159265f) th -= 3.14159265f;
+        const float ux = lxy > 0.f ? dx / lxy : 1.f, uy = lxy > 0.f ? dy / lxy : 0.f;
+        const float rad = 0.5f * sqrtf(sx * sx + sy * sy) + 1e-6f;
+        const float perp = (x1 * uy - y1 * ux) / rad;                 // [-1, 1] for lines through the grid
+        const float along = -(x1 * ux + y1 * uy);                     // parameter (in-plane length) of the centre
+        const float slope = lxy > 0.f ? dz / lxy : 0.f;
+        const float zc = (z1 + slope * along) / (sz + 1e-6f);         // about [-0.5, 0.5] inside
+        auto q = [](float v, float lo, float hi, int bits) {
+            const float f = fminf(fmaxf((v - lo) / (hi - lo), 0.f), 1.f);
+            return (unsigned)fminf(f * (float)(1 << bits), (float)((1 << bits) - 1));
+        };
+        const unsigned k = (xdrive << 30) | (q(th, 0.f, 3.14159265f, 8) << 22) | (q(perp, -1.f, 1.f, 8) << 14) |
+                           (q(zc, -1.f, 1.f, 7) << 7) | q(atanf(slope), -1.5708f, 1.5708f, 7);
+        keys[i] = (int32_t)k;
     }
 }
 
@@ -470,7 +510,7 @@ static nefct_status cb_backward_impl(const nefct_cb_geom *g, const T *sino, T *v
 
 template <typename T>
 static nefct_status lor_impl(const nefct_grid *grid, const T *lors, int64_t n, const T *src, T *dst,
-                             uint32_t flags, cudaStream_t s, bool forward)
+                             uint32_t flags, cudaStream_t s, bool forward, const int32_t *order = nullptr)
 {
     if (!grid) return fail(NEFCT_ERR_INVALID, "grid is NULL");
     nefct_status st = check_grid(*grid);
@@ -483,7 +523,8 @@ static nefct_status lor_impl(const nefct_grid *grid, const T *lors, int64_t n, c
     if (!dst) return fail(NEFCT_ERR_INVALID, "NULL output");
     LorParams<T> p;
     p.g = make_grid_dev<T>(*grid);
-    p.lors = lors; p.n = n; p.flags = flags;
+    p.lors = lors; p.n = n; p.flags = flags; p.order = order;
+    if (n >= (1ll << 31) && order) return fail(NEFCT_ERR_INVALID, "ordered walks take fewer than 2^31 lines");
     if (!forward) {
         const size_t nvox = (size_t)grid->nx * grid->ny * grid->nz;
         NEFCT_CHECK_CUDA(cudaMemsetAsync(dst, 0, nvox * sizeof(T), s));
@@ -656,6 +697,38 @@ nefct_status nefct_lor_backward(const nefct_grid *grid, const float *lors, int64
                                 float *vol, uint32_t flags, void *stream)
 {
     return lor_impl<float>(grid, lors, n, vals, vol, flags, (cudaStream_t)stream, false);
+}
+
+nefct_status nefct_lor_order_keys(const nefct_grid *grid, const float *lors, int64_t n, int32_t *keys, void *stream)
+{
+    if (!grid) return fail(NEFCT_ERR_INVALID, "grid is NULL");
+    nefct_status st = check_grid(*grid);
+    if (st) return st;
+    if (n < 0 || n >= (1ll << 31)) return fail(NEFCT_ERR_INVALID, "line count must be in [0, 2^31)");
+    if (n == 0) return NEFCT_OK;
+    if (!lors || !keys) return fail(NEFCT_ERR_INVALID, "NULL buffer");
+    LorParams<float> p{};
+    p.g = make_grid_dev<float>(*grid);
+    p.lors = lors;
+    p.n = n;
+    const long long blocks = std::min<long long>((n + 255) / 256, 148ll * 64);
+    lor_key_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(p, keys);
+    NEFCT_CHECK_LAUNCH("lor_key_kernel");
+    return NEFCT_OK;
+}
+
+nefct_status nefct_lor_forward_ordered(const nefct_grid *grid, const float *lors, int64_t n, const int32_t *order,
+                                       const float *vol, float *out, uint32_t flags, void *stream)
+{
+    if (!order && n > 0) return fail(NEFCT_ERR_INVALID, "order is NULL");
+    return lor_impl<float>(grid, lors, n, vol, out, flags, (cudaStream_t)stream, true, order);
+}
+
+nefct_status nefct_lor_backward_ordered(const nefct_grid *grid, const float *lors, int64_t n, const int32_t *order,
+                                        const float *vals, float *vol, uint32_t flags, void *stream)
+{
+    if (!order && n > 0) return fail(NEFCT_ERR_INVALID, "order is NULL");
+    return lor_impl<float>(grid, lors, n, vals, vol, flags, (cudaStream_t)stream, false, order);
 }
 
 // See cb_forward_static_impl: same result as nefct_cb_forward, with the

@@ -178,38 +178,77 @@ def cb_count_intersections(geom: ConeBeam, flags: int = _lib.REF_FORWARD, device
     return int(cnt.item())
 
 
+def _lor_grid(shape, center, size):
+    nx, ny, nz = shape
+    size = size if size is not None else (nx, ny, nz)
+    return _lib.Grid(nx, ny, nz, *[float(c) for c in center], *[float(s) for s in size])
+
+
+def _check_order(order, n, device):
+    if order is None:
+        return None
+    if order.dtype != torch.int32 or order.dim() != 1 or order.shape[0] != n or order.device != device:
+        raise NefctError(_lib.ERR_INVALID, "order must be an int32 permutation of the lines on their device")
+    return order.contiguous()
+
+
+def lor_order(lors: torch.Tensor, shape, center=(0.0, 0.0, 0.0), size=None) -> torch.Tensor:
+    """Walk order for a large unsorted line list: an int32 permutation that
+    groups nearly parallel neighbouring lines (pass it as ``order`` to
+    lor_forward / lor_backward; compute it once per list)."""
+    if lors.dim() != 2 or lors.shape[0] != 6:
+        raise NefctError(_lib.ERR_INVALID, "lors must be [6, n]")
+    _check_tensor(lors, tuple(lors.shape), "lors")
+    n = lors.shape[1]
+    keys = torch.empty(n, dtype=torch.int32, device=lors.device)
+    g = _lor_grid(shape, center, size)
+    with torch.cuda.device(lors.device):
+        _lib.call("nefct_lor_order_keys", C.byref(g), lors.data_ptr(), n, keys.data_ptr(), _stream(lors))
+    return torch.argsort(keys).to(torch.int32)
+
+
 def lor_forward(lors: torch.Tensor, vol: torch.Tensor, shape, center=(0.0, 0.0, 0.0), size=None,
-                flags: int = _lib.LOR_REF_FORWARD) -> torch.Tensor:
-    """cpp/siddon Projection: lors [6, n] -> line integrals [n]."""
+                flags: int = _lib.LOR_REF_FORWARD, order: torch.Tensor | None = None) -> torch.Tensor:
+    """cpp/siddon Projection: lors [6, n] -> line integrals [n] (optionally
+    walked in ``order`` from lor_order; results keep the lines' order)."""
     nx, ny, nz = shape
     _check_tensor(vol, (nz, ny, nx), "vol")
     if lors.dim() != 2 or lors.shape[0] != 6:
         raise NefctError(_lib.ERR_INVALID, "lors must be [6, n]")
     _check_tensor(lors, tuple(lors.shape), "lors")
     n = lors.shape[1]
+    order = _check_order(order, n, lors.device)
     out = torch.empty(n, dtype=torch.float32, device=vol.device)
-    size = size if size is not None else (nx, ny, nz)
-    g = _lib.Grid(nx, ny, nz, *[float(c) for c in center], *[float(s) for s in size])
+    g = _lor_grid(shape, center, size)
     with torch.cuda.device(vol.device):
-        _lib.call("nefct_lor_forward", C.byref(g), lors.data_ptr(), n, vol.data_ptr(), out.data_ptr(), flags,
-                  _stream(vol))
+        if order is None:
+            _lib.call("nefct_lor_forward", C.byref(g), lors.data_ptr(), n, vol.data_ptr(), out.data_ptr(), flags,
+                      _stream(vol))
+        else:
+            _lib.call("nefct_lor_forward_ordered", C.byref(g), lors.data_ptr(), n, order.data_ptr(),
+                      vol.data_ptr(), out.data_ptr(), flags, _stream(vol))
     return out
 
 
 def lor_backward(lors: torch.Tensor, vals: torch.Tensor, shape, center=(0.0, 0.0, 0.0), size=None,
-                 flags: int = _lib.LOR_REF_BACKPROJECT) -> torch.Tensor:
+                 flags: int = _lib.LOR_REF_BACKPROJECT, order: torch.Tensor | None = None) -> torch.Tensor:
     """cpp/siddon Backprojection: values [n] along lors [6, n] -> volume."""
     nx, ny, nz = shape
     if lors.dim() != 2 or lors.shape[0] != 6:
         raise NefctError(_lib.ERR_INVALID, "lors must be [6, n]")
     _check_tensor(lors, tuple(lors.shape), "lors")
     _check_tensor(vals, (lors.shape[1],), "vals")
+    n = lors.shape[1]
+    order = _check_order(order, n, lors.device)
     out = torch.empty((nz, ny, nx), dtype=torch.float32, device=vals.device)
-    size = size if size is not None else (nx, ny, nz)
-    g = _lib.Grid(nx, ny, nz, *[float(c) for c in center], *[float(s) for s in size])
+    g = _lor_grid(shape, center, size)
     with torch.cuda.device(vals.device):
-        _lib.call("nefct_lor_backward", C.byref(g), lors.data_ptr(), lors.shape[1], vals.data_ptr(),
-                  out.data_ptr(), flags, _stream(vals))
+        if order is None:
+            _lib.call("nefct_lor_backward", C.byref(g), lors.data_ptr(), n, vals.data_ptr(), out.data_ptr(),
+                      flags, _stream(vals))
+        else:
+            _lib.call("nefct_lor_backward_ordered", C.byref(g), lors.data_ptr(), n, order.data_ptr(),
+                      vals.data_ptr(), out.data_ptr(), flags, _stream(vals))
     return out
 
 

@@ -400,3 +400,27 @@ def test_edge_geometries_vs_restatement(cuda, oracle_lib, name, walk):
     assert_parity(out_b, ref_b, rel=1e-6, mabs=1e-5)
     miss = ref_f == 0                      # rays that miss the grid (the volume has no zero voxel)
     assert miss.any() and float(np.abs(out_f[miss]).max()) == 0.0
+
+
+def test_lor_ordered_walk_same_results(cuda):
+    """The ordered walk of a large unsorted line list returns the unordered
+    walk's forward bitwise (same per-line code, results at each line's
+    index) and its backward to float rounding; the order is a permutation."""
+    rng = np.random.default_rng(31)
+    n = 200_000
+    p1, p2 = rng.uniform(0, 2 * np.pi, n), rng.uniform(0, 2 * np.pi, n)
+    lors = np.stack([40 * np.cos(p1), 40 * np.sin(p1), rng.uniform(-15, 15, n),
+                     40 * np.cos(p2), 40 * np.sin(p2), rng.uniform(-15, 15, n)]).astype(np.float32)
+    lors[:, :7] = np.array([[0, 0, 0, 3, 0, 0]], np.float32).T          # short lines (Q4)
+    d_lors = torch.from_numpy(lors).to(cuda)
+    vol = torch.rand((20, 24, 28), device=cuda, generator=torch.Generator(device=cuda).manual_seed(3))
+    vals = torch.rand(n, device=cuda, generator=torch.Generator(device=cuda).manual_seed(4))
+    shape, size = (28, 24, 20), (56.0, 48.0, 40.0)
+    order = ops.lor_order(d_lors, shape, size=size)
+    assert order.dtype == torch.int32 and torch.equal(torch.sort(order.long()).values, torch.arange(n, device=cuda))
+    f0 = ops.lor_forward(d_lors, vol, shape, size=size)
+    f1 = ops.lor_forward(d_lors, vol, shape, size=size, order=order)
+    assert torch.equal(f0, f1)
+    b0 = ops.lor_backward(d_lors, vals, shape, size=size).double()
+    b1 = ops.lor_backward(d_lors, vals, shape, size=size, order=order).double()
+    assert float((b1 - b0).norm() / b0.norm()) < 1e-6

@@ -94,11 +94,14 @@ __global__ void __launch_bounds__(256) cb_backward_kernel(const __grid_constant_
 // One lane of a column warp (the whole warp calls it together).  has: the
 // lane has a ray r; FWD: gathers from the z-fastest copy volZ into *out;
 // otherwise reduces y times the ray's weights into the z-fastest accumulator
-// accZ.  Rays without a contribution (outside the detector, missing the
-// grid, zero value) stay in the warp's walk with every slot inactive.
-template <bool DIV, bool FWD>
+// accZ, or (FIX) as 64-bit fixed-point integers (value * weight * scale,
+// rounded) into fixZ.  Rays without a contribution (outside the detector,
+// missing the grid, zero value) stay in the warp's walk with every slot
+// inactive.
+template <bool DIV, bool FWD, bool FIX = false>
 __device__ __forceinline__ void colwarp_lane(const GridDev<float> &g, const float *r, bool has, uint32_t flags,
-                                             const float *__restrict__ volZ, float *out, float y, float *accZ)
+                                             const float *__restrict__ volZ, float *out, float y, float *accZ,
+                                             unsigned long long *fixZ = nullptr, float scale = 0.f)
 {
     Walk<float> w{};
     const bool live = has && (FWD || y != 0.f) && setup_walk(g, r, flags, w);
@@ -116,6 +119,8 @@ __device__ __forceinline__ void colwarp_lane(const GridDev<float> &g, const floa
         if (FWD) {
             const float v = live ? gather_walk<float, DIV, false, false>(w, g, volZ, (int)su, (int)sv, 1) : 0.f;
             if (has) *out = v;
+        } else if (live && FIX) {
+            scatter_walk_fixed<float, DIV, false>(w, g, fixZ, (int)su, (int)sv, 1, y, scale);
         } else if (live) {
             scatter_walk<float, DIV, false, false>(w, g, accZ, (int)su, (int)sv, 1, y);
         }
@@ -135,6 +140,14 @@ __device__ __forceinline__ void colwarp_lane(const GridDev<float> &g, const floa
         };
         col_walk_any<DIV, false>(c, L, K0, K1, KI0, KI1, g, f);
         if (has) *out = live ? acc * w.W : 0.f;
+    } else if (FIX) {
+        const float yw = y * w.W;
+        auto f = [&](const auto &s) {
+#pragma unroll
+            for (int i = 0; i < s.n; ++i)
+                if (s.ok[i]) atomicAdd(fixZ + s.idx[i], (unsigned long long)to_fixed((yw * s.r[i]) * scale));
+        };
+        col_walk_any<DIV, true>(c, L, K0, K1, KI0, KI1, g, f);
     } else {
         const float yw = y * w.W;
         auto f = [&](const auto &s) {

@@ -68,16 +68,18 @@ template <> struct FP<double> {
 };
 
 // Pairs of values updated by the same operation sequence (the two
-// transverse plane positions).  FP32 uses the paired sm_100 instructions,
-// which round each component exactly like the scalar _rn operation.
+// transverse plane positions).  Each component is rounded by its own scalar
+// _rn operation: a paired multiply followed by a paired add may be fused into
+// one paired fused multiply-add, which rounds once where the reference
+// rounds twice.
 template <typename T> struct Pair;
 template <> struct Pair<float> {
     float2 v;
     static __device__ __forceinline__ Pair make(float a, float b) { Pair p; p.v = make_float2(a, b); return p; }
     __device__ __forceinline__ float x() const { return v.x; }
     __device__ __forceinline__ float y() const { return v.y; }
-    static __device__ __forceinline__ Pair add(Pair a, Pair b) { Pair p; p.v = __fadd2_rn(a.v, b.v); return p; }
-    static __device__ __forceinline__ Pair mul(Pair a, Pair b) { Pair p; p.v = __fmul2_rn(a.v, b.v); return p; }
+    static __device__ __forceinline__ Pair add(Pair a, Pair b) { return make(__fadd_rn(a.v.x, b.v.x), __fadd_rn(a.v.y, b.v.y)); }
+    static __device__ __forceinline__ Pair mul(Pair a, Pair b) { return make(__fmul_rn(a.v.x, b.v.x), __fmul_rn(a.v.y, b.v.y)); }
 };
 template <> struct Pair<double> {
     double a_, b_;

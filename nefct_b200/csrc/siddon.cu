@@ -55,6 +55,43 @@ __global__ void __launch_bounds__(256) cb_backward_fixed_kernel(const __grid_con
     else scatter_walk_fixed<float, DIV, false>(w, p.g, p.fix, 1, p.g.nx, sw, y, scale);
 }
 
+// Column-warp variant: 64-bit fixed-point reductions into a z-fastest
+// accumulator (the same per-contribution integers as the thread walk, so the
+// integer sums and the result are bitwise the same).
+template <bool DIV>
+__global__ void __launch_bounds__(256) cb_colwarp_fixed_kernel(const __grid_constant__ CBParams<float> p)
+{
+    const int lane = threadIdx.x;
+    const int ia = blockIdx.x * blockDim.y + threadIdx.y;
+    int ib, iv;
+    if (p.band_major) { iv = blockIdx.y; ib = blockIdx.z * 32 + lane; }
+    else { ib = blockIdx.y * 32 + lane; iv = blockIdx.z; }
+    if (ia >= p.na) return;                       // uniform across the warp
+    const bool has = ib < p.nb;
+    const float y = has ? cb_sino_value(p, ia, ib, iv) : 0.f;
+    float r[6];
+    cb_ray(p, ia, has ? ib : 0, iv, r);
+    colwarp_lane<DIV, false, true>(p.g, r, has, p.flags, nullptr, nullptr, y, nullptr, p.fix, *p.fix_scale);
+}
+
+// vol[z][y][x] = accZ[y][x][z] / scale (the integer sums of the column warps)
+__global__ void __launch_bounds__(256) fixed_zfold_kernel(const unsigned long long *__restrict__ acc, int nx, int ny,
+                                                          int nz, const float *scale, float *__restrict__ vol)
+{
+    __shared__ unsigned long long tile[32][33];
+    const int y = blockIdx.z, x0 = blockIdx.x * 32, z0 = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int x = x0 + j, z = z0 + threadIdx.x;
+        if (x < nx && z < nz) tile[j][threadIdx.x] = acc[((size_t)y * nx + x) * nz + z];
+    }
+    __syncthreads();
+    const double inv = 1.0 / (double)*scale;
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int x = x0 + threadIdx.x, z = z0 + j;
+        if (x < nx && z < nz) vol[((size_t)z * ny + y) * nx + x] = (float)((double)(long long)tile[threadIdx.x][j] * inv);
+    }
+}
+
 // max |x| as float bits (non-negative floats order like their bit patterns)
 __global__ void __launch_bounds__(256) maxabs_kernel(const float *__restrict__ x, size_t n, unsigned *out)
 {
@@ -446,14 +483,29 @@ static nefct_status cb_backward_fixed_impl(const nefct_cb_geom *g, const float *
     p.fix = accN;
     p.fixT = accT;
     p.fix_scale = scale;
+    // column warps reduce everything into accN in z-fastest order
+    const bool cw = tr && cb_use_colwarp<float>(g->grid, flags & ~NEFCT_DETERMINISTIC, false);
     for (int v0 = 0; v0 < g->nv; v0 += ViewTable<float>::kMax) {
         const int nvc = std::min(ViewTable<float>::kMax, g->nv - v0);
         fill_views(p, g, v0, nvc);
         dim3 grid, block;
+        if (cw) {
+            cb_colwarp_shape(p, g->na, g->nb, nvc, grid, block);
+            if (cubic(p.g)) cb_colwarp_fixed_kernel<false><<<grid, block, 0, s>>>(p);
+            else cb_colwarp_fixed_kernel<true><<<grid, block, 0, s>>>(p);
+            NEFCT_CHECK_LAUNCH("cb_colwarp_fixed_kernel");
+            continue;
+        }
         cb_shape(p, g->na, g->nb, nvc, grid, block);
         if (cubic(p.g)) cb_backward_fixed_kernel<false><<<grid, block, 0, s>>>(p);
         else cb_backward_fixed_kernel<true><<<grid, block, 0, s>>>(p);
         NEFCT_CHECK_LAUNCH("cb_backward_fixed_kernel");
+    }
+    if (cw) {
+        dim3 grid((g->grid.nx + 31) / 32, (g->grid.nz + 31) / 32, g->grid.ny);
+        fixed_zfold_kernel<<<grid, dim3(32, 8), 0, s>>>(accN, g->grid.nx, g->grid.ny, g->grid.nz, scale, vol);
+        NEFCT_CHECK_LAUNCH("fixed_zfold_kernel");
+        return NEFCT_OK;
     }
     dim3 grid((g->grid.nx + 31) / 32, (g->grid.ny + 31) / 32, g->grid.nz);
     fixed_fold_kernel<<<grid, dim3(32, 8), 0, s>>>(accN, accT, g->grid.nx, g->grid.ny, scale, vol);

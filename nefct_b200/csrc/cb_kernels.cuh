@@ -161,8 +161,10 @@ __device__ __forceinline__ void colwarp_lane(const GridDev<float> &g, const floa
 
 // Column warps: warp = rows [32*tile, 32*tile + 32) of column ia at view iv,
 // over the z-fastest copy p.volT (forward, into p.out) or accumulator p.outT.
+// (at most 64 registers: 4 CTAs of 256 threads per SM; measured faster than
+// the unconstrained 70)
 template <bool DIV, bool FWD>
-__global__ void __launch_bounds__(256) cb_colwarp_kernel(const __grid_constant__ CBParams<float> p)
+__global__ void __launch_bounds__(256, 4) cb_colwarp_kernel(const __grid_constant__ CBParams<float> p)
 {
     const int lane = threadIdx.x;
     const int ia = blockIdx.x * blockDim.y + threadIdx.y;

@@ -31,6 +31,7 @@
 
 namespace nefct {
 
+
 // v part of one slab: biased bases of the low/high v voxel columns (index of
 // (k, v, z) = b + floor bits of z), the clamped v floors for the boundary
 // checks, and the v crossing ratio.
@@ -178,7 +179,7 @@ __device__ __forceinline__ void col_range(int a, int b, int kc, float &t, const 
                                           const ColEntry &e, const GridDev<float> &g, Fn &f)
 {
     const bool zdiv = g.dz != 1.f;
-#pragma unroll 2
+#pragma unroll 4
     for (int k = a; k <= b; ++k) {
         const float t2 = __fadd_rn(t, 1.f);
         t = t2;

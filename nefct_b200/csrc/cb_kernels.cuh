@@ -126,7 +126,7 @@ __device__ __forceinline__ void colwarp_lane(const GridDev<float> &g, const floa
         }
         return;
     }
-    if (FWD) {
+    if constexpr (FWD) {
         float acc = 0.f;
         // interior slabs load every slot unpredicated: an inactive slot has
         // ratio 0 and a valid index (so a volume holding +-inf may give NaN
@@ -140,7 +140,7 @@ __device__ __forceinline__ void colwarp_lane(const GridDev<float> &g, const floa
         };
         col_walk_any<DIV, false>(c, L, K0, K1, KI0, KI1, g, f);
         if (has) *out = live ? acc * w.W : 0.f;
-    } else if (FIX) {
+    } else if constexpr (FIX) {
         const float yw = y * w.W;
         auto f = [&](const auto &s) {
 #pragma unroll

@@ -10,10 +10,11 @@
 // One warp walks 32 consecutive rows of one column in lockstep over the
 // union of their slab ranges:
 //  * the v part of each slab is computed once per warp: lane j builds the
-//    entry of slab kc + j of a 32-slab chunk, and each slab's entry is
-//    broadcast with shuffles; whether the slab crosses a v plane is the same
-//    for the whole warp, so the common case without a crossing takes a
-//    two-slot split without divergence;
+//    entry of slab kc + j of a 32-slab chunk into the warp's table in shared
+//    memory, and every lane reads each slab's entry with one broadcast load;
+//    whether the slab crosses a v plane is the same for the whole warp, so
+//    the common case without a crossing takes a two-slot split without
+//    divergence;
 //  * each lane evaluates the z part and the three-voxel split of its own
 //    ray exactly as the single-ray walker does (same operations, same order);
 //  * the volume (forward) and the accumulator (transpose) are z-fastest
@@ -39,6 +40,14 @@ struct ColEntry {
     unsigned b1, b2;    // k*su + c*sv - 0x4B400000 for the low/high v floor c
     unsigned cv;        // (c1 + 2) | (c2 + 2) << 16, c clamped to [-2, nv + 1]
     float rv;           // crossing ratio, 1 without a v crossing
+};
+
+// Warp's table of the slab entries of one 32-slab chunk: .x b1, .y b2,
+// .z rv (bits), .w the slab's exit plane offset t + 1 - pu (bits); the
+// packed v floors (cv) apart, read by boundary slabs only.
+struct ColTable {
+    uint4 e[32];
+    unsigned cv[32];
 };
 
 // Shared (warp-uniform) parameters of the column's walk.
@@ -104,13 +113,14 @@ template <int NS, bool CHK> struct ColSlots {
 // general split for every slab (no branch: the forward's loads of
 // consecutive slabs interleave better).  f(slots) consumes.
 template <bool DIV, bool CHECK, int WUP, bool SPLIT, class Fn>
-__device__ __forceinline__ void col_slab(ColLane &L, float d, float dz, bool zdiv, float nz2, int nv, int nz,
-                                         const ColEntry &e, int j, Fn &f)
+__device__ __forceinline__ void col_slab(ColLane &L, float dz, bool zdiv, float nz2, int nv, int nz,
+                                         const ColTable &tab, int j, Fn &f)
 {
-    const unsigned b1 = __shfl_sync(0xffffffffu, e.b1, j);
-    const unsigned b2 = __shfl_sync(0xffffffffu, e.b2, j);
+    const uint4 te = tab.e[j];          // same address for every lane: one broadcast
+    const unsigned b1 = te.x, b2 = te.y;
+    const float d = __uint_as_float(te.w);
     unsigned cv = 0;
-    if (CHECK) cv = __shfl_sync(0xffffffffu, e.cv, j);
+    if (CHECK) cv = tab.cv[j];
 
     float qbw = __fadd_rn(L.pw, __fmul_rn(L.kw, d));
     if (DIV && zdiv) qbw = __fdiv_rn(qbw, dz);
@@ -145,7 +155,7 @@ __device__ __forceinline__ void col_slab(ColLane &L, float d, float dz, bool zdi
         }
         f(s);
     } else {
-        const float rv = __shfl_sync(0xffffffffu, e.rv, j);
+        const float rv = __uint_as_float(te.z);
         const bool vx = SPLIT || b1 != b2;
         const bool vfirst = rv > rw;
         ColSlots<3, CHECK> s;
@@ -173,28 +183,28 @@ __device__ __forceinline__ void col_slab(ColLane &L, float d, float dz, bool zdi
 }
 
 // Walks slabs [a, b] (inside the current 32-slab chunk starting at kc) in
-// one check mode.  t is the entry plane k - nu2 of slab k, carried exactly.
+// one check mode.
 template <bool DIV, bool CHECK, int WUP, bool SPLIT, class Fn>
-__device__ __forceinline__ void col_range(int a, int b, int kc, float &t, const ColShared &c, ColLane &L,
-                                          const ColEntry &e, const GridDev<float> &g, Fn &f)
+__device__ __forceinline__ void col_range(int a, int b, int kc, const ColShared &c, ColLane &L,
+                                          const ColTable &tab, const GridDev<float> &g, Fn &f)
 {
     const bool zdiv = g.dz != 1.f;
 #pragma unroll 4
-    for (int k = a; k <= b; ++k) {
-        const float t2 = __fadd_rn(t, 1.f);
-        t = t2;
-        col_slab<DIV, CHECK, WUP, SPLIT>(L, __fsub_rn(t2, c.pu), g.dz, zdiv, g.nz2, c.nv, g.nz, e, k - kc, f);
-    }
+    for (int k = a; k <= b; ++k)
+        col_slab<DIV, CHECK, WUP, SPLIT>(L, g.dz, zdiv, g.nz2, c.nv, g.nz, tab, k - kc, f);
 }
 
 // Slabs [K0, K1] of the warp in 32-slab chunks (lane j builds the entry of
-// slab kc + j); boundary slabs outside [KI0, KI1] with range checks.
+// slab kc + j into the warp's table); boundary slabs outside [KI0, KI1] with
+// range checks.  The slab planes k - nu2 and k + 1 - nu2 are exact (nu2 is a
+// multiple of 1/2 and |k| < 2^22), so the table's exit plane offset equals
+// the one a walk carrying t += 1 evaluates.
 template <bool DIV, int WUP, bool SPLIT, class Fn>
 __device__ __forceinline__ void col_walk(const ColShared &c, ColLane &L, int K0, int K1, int KI0, int KI1,
-                                         const GridDev<float> &g, Fn &f)
+                                         const GridDev<float> &g, ColTable &tab, Fn &f)
 {
     // plane K0 - nu2 (entry plane of the first slab)
-    float t = __fsub_rn((float)K0, c.nu2);
+    const float t = __fsub_rn((float)K0, c.nu2);
     float q = __fadd_rn(L.pw, __fmul_rn(L.kw, __fsub_rn(t, c.pu)));
     if (DIV && g.dz != 1.f) q = __fdiv_rn(q, g.dz);
     L.qaw = __fadd_rn(q, g.nz2);
@@ -203,10 +213,15 @@ __device__ __forceinline__ void col_walk(const ColShared &c, ColLane &L, int K0,
     if (KI0 > KI1) { KI0 = K1 + 1; KI1 = K1; }      // no interior: everything checked
     for (int kc = K0; kc <= K1; kc += 32) {
         const ColEntry e = col_entry<DIV>(c, kc + lane);
+        const float d = __fsub_rn(__fadd_rn(__fsub_rn((float)(kc + lane), c.nu2), 1.f), c.pu);
+        __syncwarp();                   // the previous chunk's reads are done
+        tab.e[lane] = make_uint4(e.b1, e.b2, __float_as_uint(e.rv), __float_as_uint(d));
+        tab.cv[lane] = e.cv;
+        __syncwarp();
         const int ke = min(K1, kc + 31);
-        col_range<DIV, true, WUP, SPLIT>(kc, min(ke, KI0 - 1), kc, t, c, L, e, g, f);
-        col_range<DIV, false, WUP, SPLIT>(max(kc, KI0), min(ke, KI1), kc, t, c, L, e, g, f);
-        col_range<DIV, true, WUP, SPLIT>(max(kc, KI1 + 1), ke, kc, t, c, L, e, g, f);
+        col_range<DIV, true, WUP, SPLIT>(kc, min(ke, KI0 - 1), kc, c, L, tab, g, f);
+        col_range<DIV, false, WUP, SPLIT>(max(kc, KI0), min(ke, KI1), kc, c, L, tab, g, f);
+        col_range<DIV, true, WUP, SPLIT>(max(kc, KI1 + 1), ke, kc, c, L, tab, g, f);
     }
 }
 
@@ -214,11 +229,14 @@ template <bool DIV, bool SPLIT, class Fn>
 __device__ __forceinline__ void col_walk_any(const ColShared &c, ColLane &L, int K0, int K1, int KI0, int KI1,
                                              const GridDev<float> &g, Fn &f)
 {
+    // one table per warp; column-warp blocks are 32 x (at most 8) threads
+    __shared__ ColTable tables[8];
+    ColTable &tab = tables[threadIdx.y];
     const bool all_up = __all_sync(0xffffffffu, L.up || !L.live);
     const bool all_down = __all_sync(0xffffffffu, !L.up || !L.live);
-    if (all_up) col_walk<DIV, 1, SPLIT>(c, L, K0, K1, KI0, KI1, g, f);
-    else if (all_down) col_walk<DIV, 0, SPLIT>(c, L, K0, K1, KI0, KI1, g, f);
-    else col_walk<DIV, 2, SPLIT>(c, L, K0, K1, KI0, KI1, g, f);
+    if (all_up) col_walk<DIV, 1, SPLIT>(c, L, K0, K1, KI0, KI1, g, tab, f);
+    else if (all_down) col_walk<DIV, 0, SPLIT>(c, L, K0, K1, KI0, KI1, g, tab, f);
+    else col_walk<DIV, 2, SPLIT>(c, L, K0, K1, KI0, KI1, g, tab, f);
 }
 
 // Strides of the z-fastest layout [y][x][z] along (u, v) of the drive axis.

@@ -257,9 +257,10 @@ nefct_status nefct_lor_backward_ordered(const nefct_grid *grid, const float *lor
  * Follows mat_codes/filtering.m:5-48 and ParkerWeight.m:5-27 with DSD =
  * src_det, DSO = src_iso, du = da, dv = db, u along detector columns.
  * parker: 0 off, +1 / -1 on with ParkerWeight's `dir` = +1 / -1 (the view
- * step is taken from angles[1] - angles[0]).  The zero-padded FFT
- * convolution of the MATLAB code is evaluated as the equal direct linear
- * convolution with the real, even spatial kernel. */
+ * step is taken from angles[1] - angles[0]).  Like the MATLAB code, each
+ * row is zero-padded to L = max(64, 2^nextpow2(2 na)), transformed,
+ * multiplied by the windowed filter response and transformed back (FP32
+ * FFTs on the device, two rows per complex transform).  na <= 2048. */
 nefct_status nefct_fdk_filter(const nefct_cb_geom *g, const float *sino, float *out, int32_t window,
                               int32_t parker, void *stream);
 

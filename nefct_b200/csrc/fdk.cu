@@ -3,11 +3,16 @@
 //
 // Filter (mat_codes/filtering.m:5-48, ParkerWeight.m:5-27): the MATLAB code
 // zero-pads each detector row to L = max(64, 2^nextpow2(2*nu)), multiplies
-// its FFT by the windowed |FFT(ramp)|*2 and crops.  Because the row occupies
-// at most L/2 samples the circular convolution never wraps, so it equals the
-// direct linear convolution of the row with h = real(IFFT(filter)) over lags
-// -(nu-1)..(nu-1).  h is built on the host in FP64 (radix-2 FFT below) with
-// the MATLAB scale folded in; the device convolves rows out of shared memory.
+// its FFT by the windowed |FFT(ramp)|*2 and crops.  The device does the same
+// with its own FFT: two weighted rows travel as the real and imaginary parts
+// of one complex signal (the filter response H is real and even, so the two
+// filtered rows come back as the real and imaginary parts of the inverse
+// transform), forward transform, multiply by H/L, inverse transform as the
+// conjugate of a forward transform of the conjugate.  The transforms are
+// Stockham autosort FFTs (radix 4, plus one radix-2 stage when log2 L is
+// odd) in shared memory; the first stage reads the weighted rows from
+// global memory and the last writes the filtered rows.  H is built on the
+// host in FP64 (radix-2 FFT below) with the MATLAB scale folded in.
 //
 // Backprojection (nefct/cc/pixel_3d/pixel.cu.cc:12-146 geometry and index
 // rules, Q9-Q11, times (src_iso/(src_iso + x'))^2 from
@@ -16,6 +21,7 @@
 // column and magnification once and then the kZ row taps (one fused
 // multiply-add, an exact floor and four gathers per voxel and view).  Views are
 // processed in chunks so a chunk's filtered projections stay in L2.
+#include <limits.h>
 #include <math.h>
 #include <algorithm>
 #include <complex>
@@ -55,12 +61,20 @@ static void fft_inplace(std::vector<std::complex<double>> &a, bool inverse)
         for (auto &x : a) x /= (double)n;
 }
 
-// h_lin[d + na - 1], d = -(na-1)..(na-1): the linear-convolution taps.
-static std::vector<float> ramp_taps(int na, int window, double scale)
+// Transform length of filtering.m: L = max(64, 2^nextpow2(2*nu)).
+static int ramp_length(int na)
 {
     int p = 0;
-    while ((1 << p) < 2 * na) ++p;                      // nextpow2(2*nu)
-    const int L = std::max(64, 1 << p);
+    while ((1 << p) < 2 * na) ++p;
+    return std::max(64, 1 << p);
+}
+
+// H[k] * scale / L for k = 0..L/2 (H[L - k] = H[k]): the windowed filter
+// response of filtering.m:54-88 with its scale and the inverse transform's
+// 1/L folded in.
+static std::vector<float> ramp_response(int na, int window, double scale)
+{
+    const int L = ramp_length(na);
     // ramp_flat (filtering.m:54-60): nn = -L/2..L/2-1, 1/4 at 0, -1/(pi nn)^2 at odd nn
     std::vector<std::complex<double>> r(L);
     for (int i = 0; i < L; ++i) {
@@ -71,8 +85,8 @@ static std::vector<float> ramp_taps(int na, int window, double scale)
         r[i] = v;
     }
     fft_inplace(r, false);
-    // Filter (:63-88): 2|FFT|, window on bins 1..L/2, mirror to length L
-    std::vector<double> filt(L / 2 + 1);
+    // Filter (:63-88): 2|FFT|, window on bins 1..L/2 (mirrored to length L)
+    std::vector<float> h(L / 2 + 1);
     for (int k = 0; k <= L / 2; ++k) {
         double f = 2.0 * std::abs(r[k]);
         const double w = 2.0 * M_PI * k / L;
@@ -86,112 +100,209 @@ static std::vector<float> ramp_taps(int na, int window, double scale)
             }
         }
         if (w > M_PI) f = 0.0;
-        filt[k] = f;
+        h[k] = (float)(f * scale / L);
     }
-    std::vector<std::complex<double>> full(L);
-    for (int k = 0; k <= L / 2; ++k) full[k] = filt[k];
-    for (int k = 1; k < L / 2; ++k) full[L - k] = filt[k];
-    fft_inplace(full, true);
-    std::vector<float> taps(2 * na - 1);
-    for (int d = -(na - 1); d <= na - 1; ++d) taps[d + na - 1] = (float)(full[(d + L) % L].real() * scale);
-    return taps;
+    return h;
 }
 
-// ---------------- device: weighting + row convolution ----------------
+// ---------------- device: weighting + FFT filtering ----------------
 
-static constexpr int kMaxCols = 2048;   // detector columns the filter supports
+static constexpr int kMaxCols = 2048;            // detector columns the filter supports
+static constexpr int kMaxL = 4096;               // ramp_length(kMaxCols)
+static constexpr int kFftThreads = 256;
 
 struct FilterParams {
-    int na, nb, nv;
-    double src_det;           // DSD
-    double da, a_shift, db, b_shift;
-    int parker;               // 0 off, +1/-1 = ParkerWeight dir
-    double dang;              // view step, degrees
-    double fanang;            // ParkerWeight's fanang (half the fan angle), degrees
-    float taps[2 * kMaxCols - 1];  // h[d + na - 1], scale folded in (kernel parameter space)
+    int na, nb, nv, L, log2L, pairs_per_view, pairs;
+    float src_det, da, a_shift, db, b_shift;    // cosine weight (FP32)
+    double src_det_d, da_d, a_shift_d;          // Parker weight (FP64, as ParkerWeight.m)
+    int parker;                                 // 0 off, +1/-1 = ParkerWeight dir
+    double dang;                                // view step, degrees
+    double fanang;                              // ParkerWeight's fanang (half the fan angle), degrees
+    float h[kMaxL / 2 + 1];                     // H[k] * scale / L, k = 0..L/2
 };
 
-static constexpr int kFiltThreads = 128;   // each thread owns 4 consecutive outputs per group
-static constexpr int kFiltRows = 4;        // detector rows per CTA (the taps are staged once)
+// Shared-memory index of element e of a transform buffer: one float2 of
+// padding per 16 spreads the strided writes of the early Stockham stages
+// over the banks.
+__host__ __device__ __forceinline__ int fpad(int e) { return e + (e >> 4); }
 
-// Shared-memory layout of the filter: taps h[d] for d in [-8, 2na + 8) at
-// hs[d + kHPad + off] (zero outside [0, 2na - 2]), off in 0..3 chosen so that
-// a thread's tap window starts on a 16-byte boundary; then the weighted row
-// x[0..na) with a zero tail to a multiple of 4.
-static constexpr int kHPad = 8;
-__host__ __device__ static inline int filt_h_floats(int na) { return (2 * na + 2 * kHPad + 4 + 3) & ~3; }
-static inline size_t filt_smem_bytes(int na) { return (size_t)(filt_h_floats(na) + ((na + 3) & ~3) + 4) * sizeof(float); }
-
-__global__ void __launch_bounds__(kFiltThreads) fdk_filter_kernel(const __grid_constant__ FilterParams p,
-                                                                  const float *__restrict__ sino,
-                                                                  float *__restrict__ out)
+// Shared memory: two padded L-point complex buffers (ping-pong), the
+// twiddle tables of the radix-4 stages (stage with Ns points per finished
+// sub-transform: W^(r k L/(4 Ns)) at [Ns - 1 or Ns - 2 + (r - 1) Ns + k],
+// 3 Ns entries, fewer than L in all) and H[0..L/2].
+static inline size_t filt_smem_bytes(int L)
 {
-    extern __shared__ __align__(16) float sm[];
-    const int na = p.na;
-    const int off = (5 - na) & 3;                     // (na - 5 + off) % 4 == 0
-    const int hn = filt_h_floats(na);
-    float *hs = sm;
-    float *x = sm + hn;
-    const int na4 = (na + 3) & ~3;
-    for (int i = threadIdx.x; i < hn; i += blockDim.x) {
-        const int d = i - kHPad - off;
-        hs[i] = (d >= 0 && d <= 2 * na - 2) ? p.taps[d] : 0.f;
+    return (size_t)(2 * fpad(L) + L) * sizeof(float2) + (size_t)(L / 2 + 4) * sizeof(float);
+}
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b)
+{
+    return make_float2(fmaf(a.x, b.x, -(a.y * b.y)), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// (-i) * a
+__device__ __forceinline__ float2 cmul_mi(float2 a) { return make_float2(a.y, -a.x); }
+
+// Cosine weight of detector element (row, col), filtering.m:10.
+// (DSD * rsqrt: a few ulp, against the FP64 of the MATLAB code)
+__device__ __forceinline__ float cos_weight(const FilterParams &p, int row, int col)
+{
+    const float u = __fsub_rn(__fmul_rn((float)col + p.a_shift, p.da), __fmul_rn((float)p.na, p.da) * 0.5f);
+    const float v = __fsub_rn(__fmul_rn((float)row + p.b_shift, p.db), __fmul_rn((float)p.nb, p.db) * 0.5f);
+    return p.src_det * rsqrtf(__fadd_rn(__fadd_rn(__fmul_rn(p.src_det, p.src_det), __fmul_rn(u, u)), __fmul_rn(v, v)));
+}
+
+// Parker weight of detector column col at view iv, ParkerWeight.m:5-25
+// (1-based views there), in FP64 as the MATLAB code.
+__device__ __forceinline__ float parker_weight(const FilterParams &p, int iv, int col)
+{
+    const double ud = ((double)col + p.a_shift_d) * p.da_d - (double)p.na * p.da_d / 2.0;
+    const double as = atan(ud / p.src_det_d) / M_PI * 180.0;
+    const double f = p.fanang;
+    const double n180 = 180.0 / p.dang;
+    const double pw = ((n180 - p.nv) / 2.0 + (iv + 1)) / n180 * 180.0 + p.parker * as;
+    double pk = 1.0;
+    if (pw <= f / 2 && pw > -f / 2) {
+        const double sn = fmax(sin(M_PI / 2 * (f / 2 + pw) / f), 0.0);
+        pk = sn * sn;
     }
-    const int iv = blockIdx.y;
-    for (int row = blockIdx.x * kFiltRows; row < min(p.nb, (blockIdx.x + 1) * kFiltRows); ++row) {
-        __syncthreads();                                  // taps staged / previous row consumed
-        const double v = ((double)row + p.b_shift) * p.db - (double)p.nb * p.db / 2.0;
-        const float *src = sino + ((size_t)iv * p.nb + row) * na;
-        for (int j = threadIdx.x; j < na4; j += blockDim.x) {
-            if (j >= na) { x[j] = 0.f; continue; }
-            const double u = ((double)j + p.a_shift) * p.da - (double)na * p.da / 2.0;
-            // cosine weight, filtering.m:10
-            double w = p.src_det / sqrt(p.src_det * p.src_det + u * u + v * v);
-            if (p.parker) {
-                // ParkerWeight.m:5-25 (view i is 1-based there)
-                const double as = atan(u / p.src_det) / M_PI * 180.0;
-                const double f = p.fanang;
-                const double n180 = 180.0 / p.dang;
-                const double pw = ((n180 - p.nv) / 2.0 + (iv + 1)) / n180 * 180.0 + p.parker * as;
-                if (pw <= f / 2 && pw > -f / 2) {
-                    const double s = fmax(sin(M_PI / 2 * (f / 2 + pw) / f), 0.0);
-                    w *= s * s;
-                }
-                if (pw >= 180 - f / 2 && pw < 180 + f / 2) {
-                    const double c = fmax(cos(M_PI / 2 * (f / 2 + pw - 180) / f), 0.0);
-                    w *= c * c;
-                }
-                if (pw < -f / 2 || pw > 180 + f / 2) w = 0.0;
-            }
-            x[j] = (float)((double)src[j] * w);
+    if (pw >= 180 - f / 2 && pw < 180 + f / 2) {
+        const double c = fmax(cos(M_PI / 2 * (f / 2 + pw - 180) / f), 0.0);
+        pk *= c * c;
+    }
+    if (pw < -f / 2 || pw > 180 + f / 2) pk = 0.0;
+    return (float)pk;
+}
+
+// One Stockham stage of radix R (2 or 4) with Ns = 2^lNs points per
+// finished sub-transform: butterfly j (< L/R) reads elements j + r L/R,
+// multiplies them by W^(r k L/(R Ns)) (k = j mod Ns; radix 4 only, from
+// the stage's table tws), transforms them and writes them to
+// (j - k) R + k + r Ns.  load(e) gives the input element e, store(e, value)
+// takes the output element.
+template <int R, class Load, class Store>
+__device__ __forceinline__ void fft_stage(int log2L, int lNs, const float2 *tws, Load load, Store store)
+{
+    constexpr int lR = R == 2 ? 1 : 2;
+    const int LR = 1 << (log2L - lR), Ns = 1 << lNs;
+    for (int j = threadIdx.x; j < LR; j += blockDim.x) {
+        const int k = j & (Ns - 1);
+        float2 a[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) a[r] = load(j + r * LR);
+        const int o = ((j - k) << lR) + k;
+        if constexpr (R == 2) {
+            store(o, cadd(a[0], a[1]));           // the radix-2 stage is the first (Ns = 1)
+            store(o + Ns, csub(a[0], a[1]));
+        } else {
+#pragma unroll
+            for (int r = 1; r < 4; ++r) a[r] = cmul(a[r], tws[(r - 1) * Ns + k]);
+            const float2 t0 = cadd(a[0], a[2]), t1 = csub(a[0], a[2]);
+            const float2 t2 = cadd(a[1], a[3]), t3 = cmul_mi(csub(a[1], a[3]));
+            store(o, cadd(t0, t2));
+            store(o + Ns, cadd(t1, t3));
+            store(o + 2 * Ns, csub(t0, t2));
+            store(o + 3 * Ns, csub(t1, t3));
         }
+    }
+}
+
+// Stages of a length-2^log2L transform: one radix-2 stage first when
+// log2L is odd, radix 4 after.
+__host__ __device__ __forceinline__ int fft_stages(int log2L) { return (log2L & 1) ? 1 + (log2L - 1) / 2 : log2L / 2; }
+
+// Offset of the twiddle table of the radix-4 stage with Ns points per
+// finished sub-transform (Ns = 4^i, or 2 * 4^i after a radix-2 stage).
+__device__ __forceinline__ int tw_offset(int Ns, bool odd) { return odd ? Ns - 2 : Ns - 1; }
+
+// Forward FFT of length L = 2^log2L: the first stage reads through
+// first(e), the last writes through last(e, value), the stages between
+// ping-pong in shared memory (padded indices): stage 0 writes b1, stage 1
+// b0, and so on.
+template <class First, class Last>
+__device__ __forceinline__ void fft_run(int log2L, const float2 *tw, float2 *b0, float2 *b1, First first, Last last)
+{
+    const bool odd = log2L & 1;
+    const int nst = fft_stages(log2L);
+    auto to_b1 = [&](int e, float2 v) { b1[fpad(e)] = v; };
+    if (odd) fft_stage<2>(log2L, 0, tw, first, to_b1);
+    else fft_stage<4>(log2L, 0, tw + tw_offset(1, false), first, to_b1);
+    __syncthreads();
+    int lNs = odd ? 1 : 2;
+    float2 *src = b1, *dst = b0;
+    for (int st = 1; st < nst - 1; ++st) {
+        const float2 *tws = tw + tw_offset(1 << lNs, odd);
+        fft_stage<4>(log2L, lNs, tws, [&](int e) { return src[fpad(e)]; },
+                     [&](int e, float2 v) { dst[fpad(e)] = v; });
         __syncthreads();
-        float *dst = out + ((size_t)iv * p.nb + row) * na;
-        // out[i] = sum_j x[j] h[i - j + na - 1], j ascending for every i.  A
-        // thread owns i0..i0+3; per block of four j it needs the taps
-        // h[D-3..D+3] (D = i0 + na - 1 - j0), held in an 8-wide register
-        // window w[k] = h[D - 4 + k] that slides by four per block (one
-        // 16-byte load), with the four x[j] broadcast by one 16-byte load.
-        for (int i0 = 4 * threadIdx.x; i0 < na; i0 += 4 * blockDim.x) {
-            float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-            const float *hp = hs + kHPad + off + (i0 + na - 5);    // &h[D - 4] for j0 = 0 (16-byte aligned)
-            float4 lo = *reinterpret_cast<const float4 *>(hp);     // w0..w3
-            float4 hi = *reinterpret_cast<const float4 *>(hp + 4); // w4..w7
-            for (int j0 = 0; j0 < na4; j0 += 4) {
-                const float4 xv = *reinterpret_cast<const float4 *>(x + j0);
-                a0 = fmaf(xv.x, hi.x, a0); a0 = fmaf(xv.y, lo.w, a0); a0 = fmaf(xv.z, lo.z, a0); a0 = fmaf(xv.w, lo.y, a0);
-                a1 = fmaf(xv.x, hi.y, a1); a1 = fmaf(xv.y, hi.x, a1); a1 = fmaf(xv.z, lo.w, a1); a1 = fmaf(xv.w, lo.z, a1);
-                a2 = fmaf(xv.x, hi.z, a2); a2 = fmaf(xv.y, hi.y, a2); a2 = fmaf(xv.z, hi.x, a2); a2 = fmaf(xv.w, lo.w, a2);
-                a3 = fmaf(xv.x, hi.w, a3); a3 = fmaf(xv.y, hi.z, a3); a3 = fmaf(xv.z, hi.y, a3); a3 = fmaf(xv.w, hi.x, a3);
-                hp -= 4;
-                hi = lo;
-                lo = *reinterpret_cast<const float4 *>(hp);
-            }
-            if (i0 < na) dst[i0] = a0;
-            if (i0 + 1 < na) dst[i0 + 1] = a1;
-            if (i0 + 2 < na) dst[i0 + 2] = a2;
-            if (i0 + 3 < na) dst[i0 + 3] = a3;
+        lNs += 2;
+        float2 *t = src;
+        src = dst;
+        dst = t;
+    }
+    fft_stage<4>(log2L, lNs, tw + tw_offset(1 << lNs, odd), [&](int e) { return src[fpad(e)]; }, last);
+    __syncthreads();
+}
+
+// Persistent CTAs over row pairs (view iv, rows b and b + 1).
+__global__ void __launch_bounds__(kFftThreads) fdk_filter_kernel(const __grid_constant__ FilterParams p,
+                                                                 const float *__restrict__ sino,
+                                                                 float *__restrict__ out)
+{
+    extern __shared__ __align__(16) float2 fsm[];
+    const int L = p.L, na = p.na, log2L = p.log2L;
+    const bool odd = log2L & 1;
+    float2 *b0 = fsm, *b1 = fsm + fpad(L), *tw = fsm + 2 * fpad(L);
+    float *hs = reinterpret_cast<float *>(tw + L);
+    // twiddle tables of the radix-4 stages: W^(r k L/(4 Ns)) = exp(-2 pi i r k / (4 Ns))
+    for (int Ns = odd ? 2 : 1; Ns <= L / 4; Ns *= 4) {
+        const int off = tw_offset(Ns, odd);
+        for (int i = threadIdx.x; i < 3 * Ns; i += blockDim.x) {
+            const int r = 1 + i / Ns, k = i - (r - 1) * Ns;
+            float sn, cs;
+            sincospif((float)(r * k) / (float)(2 * Ns), &sn, &cs);   // exact argument (power-of-two denominator)
+            tw[off + i] = make_float2(cs, -sn);
         }
+    }
+    for (int k = threadIdx.x; k <= L / 2; k += blockDim.x) hs[k] = p.h[k];
+    __syncthreads();
+    // the last stage of the forward transform would write b1 after an odd
+    // number of stages, b0 after an even number: keep the spectrum there
+    float2 *const z = (fft_stages(log2L) & 1) ? b1 : b0;
+    float2 *const zf = z == b0 ? b1 : b0;
+    for (int pr = blockIdx.x; pr < p.pairs; pr += gridDim.x) {
+        const int iv = pr / p.pairs_per_view;
+        const int row = 2 * (pr - iv * p.pairs_per_view);
+        const bool two = row + 1 < p.nb;
+        const float *x0 = sino + ((size_t)iv * p.nb + row) * na;
+        const float *x1 = x0 + na;
+        // forward transform of the weighted pair, zero beyond na
+        auto first = [&](int e) {
+            if (e >= na) return make_float2(0.f, 0.f);
+            const float pk = p.parker ? parker_weight(p, iv, e) : 1.f;
+            const float a = x0[e] * (cos_weight(p, row, e) * pk);
+            const float b = two ? x1[e] * (cos_weight(p, row + 1, e) * pk) : 0.f;
+            return make_float2(a, b);
+        };
+        fft_run(log2L, tw, b0, b1, first, [&](int e, float2 v) { z[fpad(e)] = v; });
+        // inverse: conj(FFT(conj(Z H / L))); its real and imaginary parts are
+        // the filtered rows.  Stage 0 reads z and writes the other buffer,
+        // so the second run starts from (z, zf) as (b0, b1).
+        auto first2 = [&](int e) {
+            const float hk = hs[e <= L / 2 ? e : L - e];
+            const float2 v = z[fpad(e)];
+            return make_float2(v.x * hk, -(v.y * hk));
+        };
+        float *const y0 = out + ((size_t)iv * p.nb + row) * na;
+        float *const y1 = y0 + na;
+        auto last2 = [&](int e, float2 v) {
+            if (e < na) {
+                y0[e] = v.x;
+                if (two) y1[e] = -v.y;
+            }
+        };
+        fft_run(log2L, tw, z, zf, first2, last2);
     }
 }
 
@@ -309,8 +420,14 @@ nefct_status nefct_fdk_filter(const nefct_cb_geom *g, const float *sino, float *
     FilterParams *pp = new FilterParams();
     FilterParams &p = *pp;
     p.na = g->na; p.nb = g->nb; p.nv = g->nv;
-    p.src_det = g->src_det;
-    p.da = g->da; p.a_shift = g->a_shift; p.db = g->db; p.b_shift = g->b_shift;
+    p.L = ramp_length(g->na);
+    p.log2L = 0;
+    while ((1 << p.log2L) < p.L) ++p.log2L;
+    p.pairs_per_view = (g->nb + 1) / 2;
+    if ((long long)p.pairs_per_view * g->nv > INT_MAX) { delete pp; return fail(NEFCT_ERR_UNSUPPORTED, "too many detector rows x views"); }
+    p.pairs = p.pairs_per_view * g->nv;
+    p.src_det = g->src_det; p.da = g->da; p.a_shift = g->a_shift; p.db = g->db; p.b_shift = g->b_shift;
+    p.src_det_d = g->src_det; p.da_d = g->da; p.a_shift_d = g->a_shift;
     p.parker = parker;
     // scale of filtering.m:43-47: /2/du * dbeta/2 * DSD/DSO
     double dbeta;
@@ -328,11 +445,20 @@ nefct_status nefct_fdk_filter(const nefct_cb_geom *g, const float *sino, float *
         dbeta = 2.0 * M_PI / g->nv;
     }
     const double scale = 1.0 / 2.0 / fabs((double)g->da) * dbeta / 2.0 * ((double)g->src_det / g->src_iso);
-    std::vector<float> taps = ramp_taps(g->na, window, scale);
-    std::copy(taps.begin(), taps.end(), p.taps);
+    const std::vector<float> h = ramp_response(g->na, window, scale);
+    std::copy(h.begin(), h.end(), p.h);
     cudaStream_t s = (cudaStream_t)stream;
-    const size_t smem = filt_smem_bytes(g->na);
-    fdk_filter_kernel<<<dim3((g->nb + kFiltRows - 1) / kFiltRows, g->nv), kFiltThreads, smem, s>>>(p, sino, out);
+    const size_t smem = filt_smem_bytes(p.L);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(fdk_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) { delete pp; return cuda_fail(e, "fdk_filter_kernel shared memory"); }
+    }
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fdk_filter_kernel, kFftThreads, smem);
+    const int blocks = std::min(p.pairs, sms * std::max(per_sm, 1));
+    if (p.pairs > 0) fdk_filter_kernel<<<(unsigned)blocks, kFftThreads, smem, s>>>(p, sino, out);
     delete pp;
     NEFCT_CHECK_LAUNCH("fdk_filter_kernel");
     return NEFCT_OK;

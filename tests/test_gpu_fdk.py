@@ -30,6 +30,22 @@ def test_filter_vs_restatement(cuda, window, parker):
     assert_parity(out, ref)
 
 
+@pytest.mark.parametrize("na,nb_", [(1, 1), (33, 5), (2048, 3)])
+def test_filter_sizes_vs_restatement(cuda, na, nb_):
+    """Transform lengths from 64 (one column) to 4096 (the widest supported
+    detector, whose transform buffers need more than 48 KB of shared memory),
+    an odd row count (the last row pair holds one row), odd log2 L (33 columns:
+    L = 128)."""
+    nv = 3
+    ang = np.linspace(0, 2 * np.pi, nv, endpoint=False).astype(np.float32)
+    g = nb.ConeBeam((8, 8, 8), ang, 300.0, 600.0, na, 0.4, nb_, 1.1)
+    sino = np.random.default_rng(na).random((nv, nb_, na), dtype=np.float32)
+    for window in ("ram-lak", "shepp-logan"):
+        out = ops.fdk_filter(torch.from_numpy(sino).to(cuda), g, window).cpu().numpy()
+        ref = ofdk.fdk_filter(sino, 600.0, 300.0, 0.4, 1.1, window=window, angles=ang)
+        assert_parity(out, ref)
+
+
 def test_pixel_backprojection_vs_reference_fixtures(cuda, golden):
     corner = golden["pixel/corner"]
     sino = torch.from_numpy(golden["pixel/sino"]).to(cuda)

@@ -144,13 +144,18 @@ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(
 // (-i) * a
 __device__ __forceinline__ float2 cmul_mi(float2 a) { return make_float2(a.y, -a.x); }
 
-// Cosine weight of detector element (row, col), filtering.m:10.
-// (DSD * rsqrt: a few ulp, against the FP64 of the MATLAB code)
-__device__ __forceinline__ float cos_weight(const FilterParams &p, int row, int col)
+// Cosine weight of filtering.m:10, DSD / sqrt(DSD^2 + v^2 + u^2), from the
+// row's part c = DSD^2 + v^2 (cos_row) and the column (FP32 with rsqrt: a
+// few ulp, against the FP64 of the MATLAB code).
+__device__ __forceinline__ float cos_row(const FilterParams &p, int row)
+{
+    const float v = __fsub_rn(__fmul_rn((float)row + p.b_shift, p.db), __fmul_rn((float)p.nb, p.db) * 0.5f);
+    return __fadd_rn(__fmul_rn(p.src_det, p.src_det), __fmul_rn(v, v));
+}
+__device__ __forceinline__ float cos_weight(const FilterParams &p, float c, int col)
 {
     const float u = __fsub_rn(__fmul_rn((float)col + p.a_shift, p.da), __fmul_rn((float)p.na, p.da) * 0.5f);
-    const float v = __fsub_rn(__fmul_rn((float)row + p.b_shift, p.db), __fmul_rn((float)p.nb, p.db) * 0.5f);
-    return p.src_det * rsqrtf(__fadd_rn(__fadd_rn(__fmul_rn(p.src_det, p.src_det), __fmul_rn(u, u)), __fmul_rn(v, v)));
+    return p.src_det * rsqrtf(__fadd_rn(c, __fmul_rn(u, u)));
 }
 
 // Parker weight of detector column col at view iv, ParkerWeight.m:5-25
@@ -225,7 +230,7 @@ __device__ __forceinline__ void fft_run(int log2L, const float2 *tw, float2 *b0,
 {
     const bool odd = log2L & 1;
     const int nst = fft_stages(log2L);
-    auto to_b1 = [&](int e, float2 v) { b1[fpad(e)] = v; };
+    auto to_b1 = [b1](int e, float2 v) { b1[fpad(e)] = v; };
     if (odd) fft_stage<2>(log2L, 0, tw, first, to_b1);
     else fft_stage<4>(log2L, 0, tw + tw_offset(1, false), first, to_b1);
     __syncthreads();
@@ -233,15 +238,18 @@ __device__ __forceinline__ void fft_run(int log2L, const float2 *tw, float2 *b0,
     float2 *src = b1, *dst = b0;
     for (int st = 1; st < nst - 1; ++st) {
         const float2 *tws = tw + tw_offset(1 << lNs, odd);
-        fft_stage<4>(log2L, lNs, tws, [&](int e) { return src[fpad(e)]; },
-                     [&](int e, float2 v) { dst[fpad(e)] = v; });
+        const float2 *const sp = src;
+        float2 *const dp = dst;
+        fft_stage<4>(log2L, lNs, tws, [sp](int e) { return sp[fpad(e)]; },
+                     [dp](int e, float2 v) { dp[fpad(e)] = v; });
         __syncthreads();
         lNs += 2;
         float2 *t = src;
         src = dst;
         dst = t;
     }
-    fft_stage<4>(log2L, lNs, tw + tw_offset(1 << lNs, odd), [&](int e) { return src[fpad(e)]; }, last);
+    const float2 *const sp = src;
+    fft_stage<4>(log2L, lNs, tw + tw_offset(1 << lNs, odd), [sp](int e) { return sp[fpad(e)]; }, last);
     __syncthreads();
 }
 
@@ -278,14 +286,15 @@ __global__ void __launch_bounds__(kFftThreads) fdk_filter_kernel(const __grid_co
         const float *x0 = sino + ((size_t)iv * p.nb + row) * na;
         const float *x1 = x0 + na;
         // forward transform of the weighted pair, zero beyond na
+        const float c0 = cos_row(p, row), c1 = cos_row(p, row + 1);
         auto first = [&](int e) {
             if (e >= na) return make_float2(0.f, 0.f);
             const float pk = p.parker ? parker_weight(p, iv, e) : 1.f;
-            const float a = x0[e] * (cos_weight(p, row, e) * pk);
-            const float b = two ? x1[e] * (cos_weight(p, row + 1, e) * pk) : 0.f;
+            const float a = x0[e] * (cos_weight(p, c0, e) * pk);
+            const float b = two ? x1[e] * (cos_weight(p, c1, e) * pk) : 0.f;
             return make_float2(a, b);
         };
-        fft_run(log2L, tw, b0, b1, first, [&](int e, float2 v) { z[fpad(e)] = v; });
+        fft_run(log2L, tw, b0, b1, first, [z](int e, float2 v) { z[fpad(e)] = v; });
         // inverse: conj(FFT(conj(Z H / L))); its real and imaginary parts are
         // the filtered rows.  Stage 0 reads z and writes the other buffer,
         // so the second run starts from (z, zf) as (b0, b1).
@@ -332,9 +341,12 @@ struct BpParams {
 // needed.  Per voxel the detector row is b = (m/db) * z + (nb/2 -
 // bi - 0.5) by one fused multiply-add (the reference's (m*z)/db + nb/2 - bi
 // - 0.5 rounds four times; the two differ by a few ulp of b, which moves the
-// bilinear weights continuously), clamped to [-2, nb + 1] (a voxel at the
-// source plane has an infinite or NaN b) and floored exactly by the
-// magic-constant sum (floor(b) + 1.5*2^23 = round-down(b + 1.5*2^23)).
+// bilinear weights continuously) and floored exactly by the magic-constant
+// sum (floor(b) + 1.5*2^23 = round-down(b + 1.5*2^23), valid for |b| < 2^22).
+// When |m/db| * max|z| + |nb/2 - bi - 0.5| could reach 2^21 (a voxel at or
+// near the source plane has an infinite or NaN b) the thread clamps b to
+// [-2, nb + 1] first.  The distance weight is folded into the column
+// weights (wa u, wa2 u) once per view.
 __global__ void __launch_bounds__(128) fdk_bp_kernel(const __grid_constant__ BpParams p,
                                                      const float *__restrict__ sino, float *__restrict__ vol)
 {
@@ -354,6 +366,9 @@ __global__ void __launch_bounds__(128) fdk_bp_kernel(const __grid_constant__ BpP
         zc[k] = (float)((iz + 0.5) * (double)p.sz / p.nz + (double)p.corner_z);
         acc[k] = (!p.first && iz < p.nz) ? vol[iz * plane + col] : 0.f;
     }
+    float zabs = 0.f;
+#pragma unroll
+    for (int k = 0; k < kZ; ++k) zabs = fmaxf(zabs, fabsf(zc[k]));
     const float xs = -p.src_iso;
     const float nah = (float)(p.na / 2);   // integer half (Q9)
     const float bhi = (float)(p.nb + 1);
@@ -378,18 +393,34 @@ __global__ void __launch_bounds__(128) fdk_bp_kernel(const __grid_constant__ BpP
             u = r * r;
         }
         const float bm = m * p.inv_db;
+        const float wau = wa * u, wa2u = wa2 * u;
         const float *pv = sino + (size_t)v * p.na * p.nb + ia;
+        if (fabsf(bm) * zabs + fabsf(p.cb) < 2097152.f) {
 #pragma unroll
-        for (int k = 0; k < kZ; ++k) {
-            const float b = fminf(fmaxf(fmaf(bm, zc[k], p.cb), -2.f), bhi);
-            const float mb = __fadd_rd(b, 12582912.0f);
-            const unsigned ib = (unsigned)(__float_as_int(mb) - 0x4B400000);
-            if (ib >= nb1) continue;                           // ib < 0 || ib + 1 >= nb
-            const float wb2 = b - __fsub_rn(mb, 12582912.0f), wb = 1.f - wb2;
-            const float *q = pv + (size_t)ib * p.na;
-            const float r0 = fmaf(__ldg(q + 1), wa2, __ldg(q) * wa);
-            const float r1 = fmaf(__ldg(q + p.na + 1), wa2, __ldg(q + p.na) * wa);
-            acc[k] = fmaf(fmaf(r1, wb2, r0 * wb), u, acc[k]);
+            for (int k = 0; k < kZ; ++k) {
+                const float b = fmaf(bm, zc[k], p.cb);
+                const float mb = __fadd_rd(b, 12582912.0f);
+                const unsigned ib = (unsigned)(__float_as_int(mb) - 0x4B400000);
+                if (ib >= nb1) continue;
+                const float wb2 = b - __fsub_rn(mb, 12582912.0f), wb = 1.f - wb2;
+                const float *q = pv + ib * p.na;
+                const float r0 = fmaf(__ldg(q + 1), wa2u, __ldg(q) * wau);
+                const float r1 = fmaf(__ldg(q + p.na + 1), wa2u, __ldg(q + p.na) * wau);
+                acc[k] = fmaf(r1, wb2, fmaf(r0, wb, acc[k]));
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < kZ; ++k) {
+                const float b = fminf(fmaxf(fmaf(bm, zc[k], p.cb), -2.f), bhi);
+                const float mb = __fadd_rd(b, 12582912.0f);
+                const unsigned ib = (unsigned)(__float_as_int(mb) - 0x4B400000);
+                if (ib >= nb1) continue;                           // ib < 0 || ib + 1 >= nb
+                const float wb2 = b - __fsub_rn(mb, 12582912.0f), wb = 1.f - wb2;
+                const float *q = pv + (size_t)ib * p.na;
+                const float r0 = fmaf(__ldg(q + 1), wa2u, __ldg(q) * wau);
+                const float r1 = fmaf(__ldg(q + p.na + 1), wa2u, __ldg(q + p.na) * wau);
+                acc[k] = fmaf(r1, wb2, fmaf(r0, wb, acc[k]));
+            }
         }
     }
 #pragma unroll

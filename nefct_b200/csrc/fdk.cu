@@ -181,87 +181,104 @@ __device__ __forceinline__ float parker_weight(const FilterParams &p, int iv, in
     return (float)pk;
 }
 
-// One Stockham stage of radix R (2 or 4) with Ns = 2^lNs points per
-// finished sub-transform: butterfly j (< L/R) reads elements j + r L/R,
-// multiplies them by W^(r k L/(R Ns)) (k = j mod Ns; radix 4 only, from
-// the stage's table tws), transforms them and writes them to
-// (j - k) R + k + r Ns.  load(e) gives the input element e, store(e, value)
-// takes the output element.
-template <int R, class Load, class Store>
-__device__ __forceinline__ void fft_stage(int log2L, int lNs, const float2 *tws, Load load, Store store)
+// One Stockham stage of radix R (2 or 4) of a length-2^LOG2L transform with
+// Ns = 2^LNS points per finished sub-transform: butterfly j (< L/R) reads
+// elements j + r L/R, multiplies them by W^(r k L/(R Ns)) (k = j mod Ns;
+// radix 4 only, from the stage's table tws), transforms them and writes
+// them to (j - k) R + k + r Ns.  load(e, i) gives element e (i = fpad(e),
+// its shared-memory index); store(e, i, value) takes output element e.  The
+// sizes are compile-time, so the index arithmetic folds into constants.
+template <int R, int LOG2L, int LNS, class Load, class Store>
+__device__ __forceinline__ void fft_stage(const float2 *tws, Load load, Store store)
 {
     constexpr int lR = R == 2 ? 1 : 2;
-    const int LR = 1 << (log2L - lR), Ns = 1 << lNs;
-    for (int j = threadIdx.x; j < LR; j += blockDim.x) {
+    constexpr int LR = 1 << (LOG2L - lR), Ns = 1 << LNS;
+    constexpr int PLR = LR + LR / 16;                  // fpad(j + r LR) = fpad(j) + r PLR (LR % 16 == 0)
+    constexpr int ITER = (LR + kFftThreads - 1) / kFftThreads;
+#pragma unroll
+    for (int it = 0; it < ITER; ++it) {
+        const int j = threadIdx.x + it * kFftThreads;
+        if (LR % kFftThreads != 0 && j >= LR) break;
         const int k = j & (Ns - 1);
+        const int pj = fpad(j);
         float2 a[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) a[r] = load(j + r * LR);
+        for (int r = 0; r < R; ++r) a[r] = load(j + r * LR, pj + r * PLR);
         const int o = ((j - k) << lR) + k;
+        auto out = [&](int r, float2 v) {
+            if constexpr (Ns >= 16) store(o + r * Ns, fpad(o) + r * (Ns + Ns / 16), v);
+            else store(o + r * Ns, fpad(o + r * Ns), v);
+        };
         if constexpr (R == 2) {
-            store(o, cadd(a[0], a[1]));           // the radix-2 stage is the first (Ns = 1)
-            store(o + Ns, csub(a[0], a[1]));
+            out(0, cadd(a[0], a[1]));            // the radix-2 stage is the first (Ns = 1)
+            out(1, csub(a[0], a[1]));
         } else {
+            if constexpr (Ns > 1) {
 #pragma unroll
-            for (int r = 1; r < 4; ++r) a[r] = cmul(a[r], tws[(r - 1) * Ns + k]);
+                for (int r = 1; r < 4; ++r) a[r] = cmul(a[r], tws[(r - 1) * Ns + k]);
+            }
             const float2 t0 = cadd(a[0], a[2]), t1 = csub(a[0], a[2]);
             const float2 t2 = cadd(a[1], a[3]), t3 = cmul_mi(csub(a[1], a[3]));
-            store(o, cadd(t0, t2));
-            store(o + Ns, cadd(t1, t3));
-            store(o + 2 * Ns, csub(t0, t2));
-            store(o + 3 * Ns, csub(t1, t3));
+            out(0, cadd(t0, t2));
+            out(1, cadd(t1, t3));
+            out(2, csub(t0, t2));
+            out(3, csub(t1, t3));
         }
     }
 }
 
 // Stages of a length-2^log2L transform: one radix-2 stage first when
 // log2L is odd, radix 4 after.
-__host__ __device__ __forceinline__ int fft_stages(int log2L) { return (log2L & 1) ? 1 + (log2L - 1) / 2 : log2L / 2; }
+__host__ __device__ constexpr int fft_stages(int log2L) { return (log2L & 1) ? 1 + (log2L - 1) / 2 : log2L / 2; }
 
 // Offset of the twiddle table of the radix-4 stage with Ns points per
 // finished sub-transform (Ns = 4^i, or 2 * 4^i after a radix-2 stage).
-__device__ __forceinline__ int tw_offset(int Ns, bool odd) { return odd ? Ns - 2 : Ns - 1; }
+__host__ __device__ constexpr int tw_offset(int Ns, bool odd) { return odd ? Ns - 2 : Ns - 1; }
 
-// Forward FFT of length L = 2^log2L: the first stage reads through
-// first(e), the last writes through last(e, value), the stages between
-// ping-pong in shared memory (padded indices): stage 0 writes b1, stage 1
-// b0, and so on.
-template <class First, class Last>
-__device__ __forceinline__ void fft_run(int log2L, const float2 *tw, float2 *b0, float2 *b1, First first, Last last)
+// Radix-4 stages from Ns = 2^LNS on: the stages before the last read src
+// and write dst in shared memory (swapping them after each stage), the
+// last (Ns = L/4) writes through last.
+template <int LOG2L, int LNS, class Last>
+__device__ __forceinline__ void fft_tail(const float2 *tw, const float2 *src, float2 *dst, Last last)
 {
-    const bool odd = log2L & 1;
-    const int nst = fft_stages(log2L);
-    auto to_b1 = [b1](int e, float2 v) { b1[fpad(e)] = v; };
-    if (odd) fft_stage<2>(log2L, 0, tw, first, to_b1);
-    else fft_stage<4>(log2L, 0, tw + tw_offset(1, false), first, to_b1);
-    __syncthreads();
-    int lNs = odd ? 1 : 2;
-    float2 *src = b1, *dst = b0;
-    for (int st = 1; st < nst - 1; ++st) {
-        const float2 *tws = tw + tw_offset(1 << lNs, odd);
-        const float2 *const sp = src;
-        float2 *const dp = dst;
-        fft_stage<4>(log2L, lNs, tws, [sp](int e) { return sp[fpad(e)]; },
-                     [dp](int e, float2 v) { dp[fpad(e)] = v; });
+    constexpr bool odd = LOG2L & 1;
+    const float2 *tws = tw + tw_offset(1 << LNS, odd);
+    auto ld = [src](int, int i) { return src[i]; };
+    if constexpr (LNS + 2 == LOG2L) {
+        fft_stage<4, LOG2L, LNS>(tws, ld, last);
         __syncthreads();
-        lNs += 2;
-        float2 *t = src;
-        src = dst;
-        dst = t;
+    } else {
+        fft_stage<4, LOG2L, LNS>(tws, ld, [dst](int, int i, float2 v) { dst[i] = v; });
+        __syncthreads();
+        fft_tail<LOG2L, LNS + 2>(tw, dst, const_cast<float2 *>(src), last);
     }
-    const float2 *const sp = src;
-    fft_stage<4>(log2L, lNs, tw + tw_offset(1 << lNs, odd), [sp](int e) { return sp[fpad(e)]; }, last);
-    __syncthreads();
 }
 
-// Persistent CTAs over row pairs (view iv, rows b and b + 1).
+// Forward FFT of length 2^LOG2L: the first stage reads through first(e, i),
+// the last writes through last(e, i, value), the stages between ping-pong
+// in shared memory (padded indices): stage 0 writes b1, stage 1 b0, ...
+template <int LOG2L, class First, class Last>
+__device__ __forceinline__ void fft_run(const float2 *tw, float2 *b0, float2 *b1, First first, Last last)
+{
+    constexpr bool odd = LOG2L & 1;
+    auto to_b1 = [b1](int, int i, float2 v) { b1[i] = v; };
+    if constexpr (odd) fft_stage<2, LOG2L, 0>(tw, first, to_b1);
+    else fft_stage<4, LOG2L, 0>(tw, first, to_b1);
+    __syncthreads();
+    fft_tail<LOG2L, odd ? 1 : 2>(tw, b1, b0, last);
+}
+
+// Persistent CTAs over row pairs (view iv, rows b and b + 1); transform
+// length 2^LOG2L.
+template <int LOG2L>
 __global__ void __launch_bounds__(kFftThreads) fdk_filter_kernel(const __grid_constant__ FilterParams p,
                                                                  const float *__restrict__ sino,
                                                                  float *__restrict__ out)
 {
+    constexpr int L = 1 << LOG2L;
+    constexpr bool odd = LOG2L & 1;
     extern __shared__ __align__(16) float2 fsm[];
-    const int L = p.L, na = p.na, log2L = p.log2L;
-    const bool odd = log2L & 1;
+    const int na = p.na;
     float2 *b0 = fsm, *b1 = fsm + fpad(L), *tw = fsm + 2 * fpad(L);
     float *hs = reinterpret_cast<float *>(tw + L);
     // twiddle tables of the radix-4 stages: W^(r k L/(4 Ns)) = exp(-2 pi i r k / (4 Ns))
@@ -278,7 +295,7 @@ __global__ void __launch_bounds__(kFftThreads) fdk_filter_kernel(const __grid_co
     __syncthreads();
     // the last stage of the forward transform would write b1 after an odd
     // number of stages, b0 after an even number: keep the spectrum there
-    float2 *const z = (fft_stages(log2L) & 1) ? b1 : b0;
+    float2 *const z = (fft_stages(LOG2L) & 1) ? b1 : b0;
     float2 *const zf = z == b0 ? b1 : b0;
     for (int pr = blockIdx.x; pr < p.pairs; pr += gridDim.x) {
         const int iv = pr / p.pairs_per_view;
@@ -288,32 +305,51 @@ __global__ void __launch_bounds__(kFftThreads) fdk_filter_kernel(const __grid_co
         const float *x1 = x0 + na;
         // forward transform of the weighted pair, zero beyond na
         const float c0 = cos_row(p, row), c1 = cos_row(p, row + 1);
-        auto first = [&](int e) {
+        auto first = [&](int e, int) {
             if (e >= na) return make_float2(0.f, 0.f);
             const float pk = p.parker ? parker_weight(p, iv, e) : 1.f;
             const float a = x0[e] * (cos_weight(p, c0, e) * pk);
             const float b = two ? x1[e] * (cos_weight(p, c1, e) * pk) : 0.f;
             return make_float2(a, b);
         };
-        fft_run(log2L, tw, b0, b1, first, [z](int e, float2 v) { z[fpad(e)] = v; });
+        fft_run<LOG2L>(tw, b0, b1, first, [z](int, int i, float2 v) { z[i] = v; });
         // inverse: conj(FFT(conj(Z H / L))); its real and imaginary parts are
         // the filtered rows.  Stage 0 reads z and writes the other buffer,
         // so the second run starts from (z, zf) as (b0, b1).
-        auto first2 = [&](int e) {
+        auto first2 = [&](int e, int i) {
             const float hk = hs[e <= L / 2 ? e : L - e];
-            const float2 v = z[fpad(e)];
+            const float2 v = z[i];
             return make_float2(v.x * hk, -(v.y * hk));
         };
         float *const y0 = out + ((size_t)iv * p.nb + row) * na;
         float *const y1 = y0 + na;
-        auto last2 = [&](int e, float2 v) {
+        auto last2 = [&](int e, int, float2 v) {
             if (e < na) {
                 y0[e] = v.x;
                 if (two) y1[e] = -v.y;
             }
         };
-        fft_run(log2L, tw, z, zf, first2, last2);
+        fft_run<LOG2L>(tw, z, zf, first2, last2);
     }
+}
+
+// Launches the filter for transform length 2^LOG2L.
+template <int LOG2L>
+static cudaError_t launch_filter(const FilterParams &p, const float *sino, float *out, cudaStream_t s)
+{
+    const size_t smem = filt_smem_bytes(1 << LOG2L);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(fdk_filter_kernel<LOG2L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fdk_filter_kernel<LOG2L>, kFftThreads, smem);
+    const int blocks = std::min(p.pairs, sms * std::max(per_sm, 1));
+    fdk_filter_kernel<LOG2L><<<blocks, kFftThreads, smem, s>>>(p, sino, out);
+    return cudaGetLastError();
 }
 
 // ---------------- device: voxel-driven backprojection ----------------
@@ -494,17 +530,20 @@ nefct_status nefct_fdk_filter(const nefct_cb_geom *g, const float *sino, float *
     const std::vector<float> h = ramp_response(g->na, window, scale);
     std::copy(h.begin(), h.end(), p.h);
     cudaStream_t s = (cudaStream_t)stream;
-    const size_t smem = filt_smem_bytes(p.L);
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(fdk_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) { delete pp; return cuda_fail(e, "fdk_filter_kernel shared memory"); }
+    cudaError_t e = cudaSuccess;
+    if (p.pairs > 0) {
+        switch (p.log2L) {
+        case 6: e = launch_filter<6>(p, sino, out, s); break;
+        case 7: e = launch_filter<7>(p, sino, out, s); break;
+        case 8: e = launch_filter<8>(p, sino, out, s); break;
+        case 9: e = launch_filter<9>(p, sino, out, s); break;
+        case 10: e = launch_filter<10>(p, sino, out, s); break;
+        case 11: e = launch_filter<11>(p, sino, out, s); break;
+        case 12: e = launch_filter<12>(p, sino, out, s); break;
+        default: delete pp; return fail(NEFCT_ERR_UNSUPPORTED, "FFT length 2^%d outside 2^6..2^12", p.log2L);
+        }
     }
-    int dev = 0, sms = 148, per_sm = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fdk_filter_kernel, kFftThreads, smem);
-    const int blocks = std::min(p.pairs, sms * std::max(per_sm, 1));
-    if (p.pairs > 0) fdk_filter_kernel<<<(unsigned)blocks, kFftThreads, smem, s>>>(p, sino, out);
+    if (e != cudaSuccess) { delete pp; return cuda_fail(e, "fdk_filter_kernel"); }
     delete pp;
     NEFCT_CHECK_LAUNCH("fdk_filter_kernel");
     return NEFCT_OK;

@@ -188,7 +188,10 @@ __device__ __forceinline__ float parker_weight(const FilterParams &p, int iv, in
 // them to (j - k) R + k + r Ns.  load(e, i) gives element e (i = fpad(e),
 // its shared-memory index); store(e, i, value) takes output element e.  The
 // sizes are compile-time, so the index arithmetic folds into constants.
-template <int R, int LOG2L, int LNS, class Load, class Store>
+// ZIN: the inputs r >= R/2 are known zero (elements >= L/2 of the padded
+// rows in the first stage); LOW: only the outputs r < R/2 are wanted
+// (elements < L/2, the cropped rows, in the last stage).
+template <int R, int LOG2L, int LNS, bool ZIN = false, bool LOW = false, class Load, class Store>
 __device__ __forceinline__ void fft_stage(const float2 *tws, Load load, Store store)
 {
     constexpr int lR = R == 2 ? 1 : 2;
@@ -203,26 +206,34 @@ __device__ __forceinline__ void fft_stage(const float2 *tws, Load load, Store st
         const int pj = fpad(j);
         float2 a[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) a[r] = load(j + r * LR, pj + r * PLR);
+        for (int r = 0; r < R; ++r) a[r] = (ZIN && r >= R / 2) ? make_float2(0.f, 0.f) : load(j + r * LR, pj + r * PLR);
         const int o = ((j - k) << lR) + k;
         auto out = [&](int r, float2 v) {
             if constexpr (Ns >= 16) store(o + r * Ns, fpad(o) + r * (Ns + Ns / 16), v);
             else store(o + r * Ns, fpad(o + r * Ns), v);
         };
         if constexpr (R == 2) {
-            out(0, cadd(a[0], a[1]));            // the radix-2 stage is the first (Ns = 1)
-            out(1, csub(a[0], a[1]));
+            if constexpr (ZIN) {                 // the radix-2 stage is the first (Ns = 1)
+                out(0, a[0]);
+                out(1, a[0]);
+            } else {
+                out(0, cadd(a[0], a[1]));
+                out(1, csub(a[0], a[1]));
+            }
         } else {
             if constexpr (Ns > 1) {
 #pragma unroll
-                for (int r = 1; r < 4; ++r) a[r] = cmul(a[r], tws[(r - 1) * Ns + k]);
+                for (int r = 1; r < 4; ++r)
+                    if (!(ZIN && r >= 2)) a[r] = cmul(a[r], tws[(r - 1) * Ns + k]);
             }
-            const float2 t0 = cadd(a[0], a[2]), t1 = csub(a[0], a[2]);
-            const float2 t2 = cadd(a[1], a[3]), t3 = cmul_mi(csub(a[1], a[3]));
+            const float2 t0 = ZIN ? a[0] : cadd(a[0], a[2]), t1 = ZIN ? a[0] : csub(a[0], a[2]);
+            const float2 t2 = ZIN ? a[1] : cadd(a[1], a[3]), t3 = cmul_mi(ZIN ? a[1] : csub(a[1], a[3]));
             out(0, cadd(t0, t2));
             out(1, cadd(t1, t3));
-            out(2, csub(t0, t2));
-            out(3, csub(t1, t3));
+            if constexpr (!LOW) {
+                out(2, csub(t0, t2));
+                out(3, csub(t1, t3));
+            }
         }
     }
 }
@@ -238,34 +249,35 @@ __host__ __device__ constexpr int tw_offset(int Ns, bool odd) { return odd ? Ns 
 // Radix-4 stages from Ns = 2^LNS on: the stages before the last read src
 // and write dst in shared memory (swapping them after each stage), the
 // last (Ns = L/4) writes through last.
-template <int LOG2L, int LNS, class Last>
+template <int LOG2L, int LNS, bool LOW, class Last>
 __device__ __forceinline__ void fft_tail(const float2 *tw, const float2 *src, float2 *dst, Last last)
 {
     constexpr bool odd = LOG2L & 1;
     const float2 *tws = tw + tw_offset(1 << LNS, odd);
     auto ld = [src](int, int i) { return src[i]; };
     if constexpr (LNS + 2 == LOG2L) {
-        fft_stage<4, LOG2L, LNS>(tws, ld, last);
+        fft_stage<4, LOG2L, LNS, false, LOW>(tws, ld, last);
         __syncthreads();
     } else {
         fft_stage<4, LOG2L, LNS>(tws, ld, [dst](int, int i, float2 v) { dst[i] = v; });
         __syncthreads();
-        fft_tail<LOG2L, LNS + 2>(tw, dst, const_cast<float2 *>(src), last);
+        fft_tail<LOG2L, LNS + 2, LOW>(tw, dst, const_cast<float2 *>(src), last);
     }
 }
 
-// Forward FFT of length 2^LOG2L: the first stage reads through first(e, i),
-// the last writes through last(e, i, value), the stages between ping-pong
-// in shared memory (padded indices): stage 0 writes b1, stage 1 b0, ...
-template <int LOG2L, class First, class Last>
+// Forward FFT of length 2^LOG2L: the first stage reads through first(e, i)
+// (ZIN: inputs e >= L/2 are zero), the last writes through last(e, i, value)
+// (LOW: outputs e < L/2 only), the stages between ping-pong in shared
+// memory (padded indices): stage 0 writes b1, stage 1 b0, ...
+template <int LOG2L, bool ZIN, bool LOW, class First, class Last>
 __device__ __forceinline__ void fft_run(const float2 *tw, float2 *b0, float2 *b1, First first, Last last)
 {
     constexpr bool odd = LOG2L & 1;
     auto to_b1 = [b1](int, int i, float2 v) { b1[i] = v; };
-    if constexpr (odd) fft_stage<2, LOG2L, 0>(tw, first, to_b1);
-    else fft_stage<4, LOG2L, 0>(tw, first, to_b1);
+    if constexpr (odd) fft_stage<2, LOG2L, 0, ZIN>(tw, first, to_b1);
+    else fft_stage<4, LOG2L, 0, ZIN>(tw, first, to_b1);
     __syncthreads();
-    fft_tail<LOG2L, odd ? 1 : 2>(tw, b1, b0, last);
+    fft_tail<LOG2L, odd ? 1 : 2, LOW>(tw, b1, b0, last);
 }
 
 // Persistent CTAs over row pairs (view iv, rows b and b + 1); transform
@@ -312,7 +324,8 @@ __global__ void __launch_bounds__(kFftThreads) fdk_filter_kernel(const __grid_co
             const float b = two ? x1[e] * (cos_weight(p, c1, e) * pk) : 0.f;
             return make_float2(a, b);
         };
-        fft_run<LOG2L>(tw, b0, b1, first, [z](int, int i, float2 v) { z[i] = v; });
+        // (rows occupy at most L/2 elements: the upper half of the input is zero)
+        fft_run<LOG2L, true, false>(tw, b0, b1, first, [z](int, int i, float2 v) { z[i] = v; });
         // inverse: conj(FFT(conj(Z H / L))); its real and imaginary parts are
         // the filtered rows.  Stage 0 reads z and writes the other buffer,
         // so the second run starts from (z, zf) as (b0, b1).
@@ -329,7 +342,8 @@ __global__ void __launch_bounds__(kFftThreads) fdk_filter_kernel(const __grid_co
                 if (two) y1[e] = -v.y;
             }
         };
-        fft_run<LOG2L>(tw, z, zf, first2, last2);
+        // (only the first na <= L/2 outputs are kept)
+        fft_run<LOG2L, false, true>(tw, z, zf, first2, last2);
     }
 }
 

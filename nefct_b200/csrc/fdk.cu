@@ -122,18 +122,28 @@ struct FilterParams {
     float h[kMaxL / 2 + 1];                     // H[k] * scale / L, k = 0..L/2
 };
 
-// Shared-memory index of element e of a transform buffer: one float2 of
-// padding per 16 spreads the strided writes of the early Stockham stages
-// over the banks.
-__host__ __device__ __forceinline__ int fpad(int e) { return e + (e >> 4); }
+// Shared-memory index of element e of a transform buffer: C float2 of
+// padding per 16 elements.  A stage writes its output with the padding that
+// keeps its strided stores free of bank conflicts (fft_cpad) and the next
+// stage reads with the same padding; loads of 16 consecutive elements are
+// conflict-free under any padding.
+template <int C> __host__ __device__ __forceinline__ int fpad(int e) { return e + C * (e >> 4); }
+
+// Padding of the output of the stage with Ns points per finished
+// sub-transform: a half-warp writes elements 4j + r (Ns = 1), 8m + k + 2r
+// (Ns = 2), 16m + k + 4r (Ns = 4) or 32m + k + 8r (Ns = 8), which C = 1, 2, 4, 4
+// spread over 16 distinct 8-byte bank pairs; for Ns >= 16 the half-warp's
+// elements are consecutive.
+__host__ __device__ constexpr int fft_cpad(int Ns) { return Ns == 1 ? 1 : Ns == 2 ? 2 : Ns <= 8 ? 4 : 1; }
 
 // Shared memory: two padded L-point complex buffers (ping-pong), the
 // twiddle tables of the radix-4 stages (stage with Ns points per finished
 // sub-transform: W^(r k L/(4 Ns)) at [Ns - 1 or Ns - 2 + (r - 1) Ns + k],
 // 3 Ns entries, fewer than L in all) and H[0..L/2].
+static constexpr int fft_buf(int L) { return L + L / 4; }   // fpad<4>(L) bound
 static inline size_t filt_smem_bytes(int L)
 {
-    return (size_t)(2 * fpad(L) + L) * sizeof(float2) + (size_t)(L / 2 + 4) * sizeof(float);
+    return (size_t)(2 * fft_buf(L) + L) * sizeof(float2) + (size_t)(L / 2 + 4) * sizeof(float);
 }
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b)
@@ -191,26 +201,27 @@ __device__ __forceinline__ float parker_weight(const FilterParams &p, int iv, in
 // ZIN: the inputs r >= R/2 are known zero (elements >= L/2 of the padded
 // rows in the first stage); LOW: only the outputs r < R/2 are wanted
 // (elements < L/2, the cropped rows, in the last stage).
-template <int R, int LOG2L, int LNS, bool ZIN = false, bool LOW = false, class Load, class Store>
+template <int R, int LOG2L, int LNS, int CIN, bool ZIN = false, bool LOW = false, class Load, class Store>
 __device__ __forceinline__ void fft_stage(const float2 *tws, Load load, Store store)
 {
     constexpr int lR = R == 2 ? 1 : 2;
     constexpr int LR = 1 << (LOG2L - lR), Ns = 1 << LNS;
-    constexpr int PLR = LR + LR / 16;                  // fpad(j + r LR) = fpad(j) + r PLR (LR % 16 == 0)
+    constexpr int COUT = fft_cpad(Ns);
+    constexpr int PLR = LR + CIN * (LR / 16);          // fpad(j + r LR) = fpad(j) + r PLR (LR % 16 == 0)
     constexpr int ITER = (LR + kFftThreads - 1) / kFftThreads;
 #pragma unroll
     for (int it = 0; it < ITER; ++it) {
         const int j = threadIdx.x + it * kFftThreads;
         if (LR % kFftThreads != 0 && j >= LR) break;
         const int k = j & (Ns - 1);
-        const int pj = fpad(j);
+        const int pj = fpad<CIN>(j);
         float2 a[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) a[r] = (ZIN && r >= R / 2) ? make_float2(0.f, 0.f) : load(j + r * LR, pj + r * PLR);
         const int o = ((j - k) << lR) + k;
         auto out = [&](int r, float2 v) {
-            if constexpr (Ns >= 16) store(o + r * Ns, fpad(o) + r * (Ns + Ns / 16), v);
-            else store(o + r * Ns, fpad(o + r * Ns), v);
+            if constexpr (Ns >= 16) store(o + r * Ns, fpad<COUT>(o) + r * (Ns + COUT * (Ns / 16)), v);
+            else store(o + r * Ns, fpad<COUT>(o + r * Ns), v);
         };
         if constexpr (R == 2) {
             if constexpr (ZIN) {                 // the radix-2 stage is the first (Ns = 1)
@@ -253,13 +264,14 @@ template <int LOG2L, int LNS, bool LOW, class Last>
 __device__ __forceinline__ void fft_tail(const float2 *tw, const float2 *src, float2 *dst, Last last)
 {
     constexpr bool odd = LOG2L & 1;
+    constexpr int CIN = fft_cpad(1 << (LNS - (LNS == 1 ? 1 : 2)));   // the previous stage's output padding
     const float2 *tws = tw + tw_offset(1 << LNS, odd);
     auto ld = [src](int, int i) { return src[i]; };
     if constexpr (LNS + 2 == LOG2L) {
-        fft_stage<4, LOG2L, LNS, false, LOW>(tws, ld, last);
+        fft_stage<4, LOG2L, LNS, CIN, false, LOW>(tws, ld, last);
         __syncthreads();
     } else {
-        fft_stage<4, LOG2L, LNS>(tws, ld, [dst](int, int i, float2 v) { dst[i] = v; });
+        fft_stage<4, LOG2L, LNS, CIN>(tws, ld, [dst](int, int i, float2 v) { dst[i] = v; });
         __syncthreads();
         fft_tail<LOG2L, LNS + 2, LOW>(tw, dst, const_cast<float2 *>(src), last);
     }
@@ -274,8 +286,10 @@ __device__ __forceinline__ void fft_run(const float2 *tw, float2 *b0, float2 *b1
 {
     constexpr bool odd = LOG2L & 1;
     auto to_b1 = [b1](int, int i, float2 v) { b1[i] = v; };
-    if constexpr (odd) fft_stage<2, LOG2L, 0, ZIN>(tw, first, to_b1);
-    else fft_stage<4, LOG2L, 0, ZIN>(tw, first, to_b1);
+    // the first stage's input index is that of the spectrum buffer (written
+    // by a last stage, Ns = L/4 >= 16: padding 1) when it is read from there
+    if constexpr (odd) fft_stage<2, LOG2L, 0, 1, ZIN>(tw, first, to_b1);
+    else fft_stage<4, LOG2L, 0, 1, ZIN>(tw, first, to_b1);
     __syncthreads();
     fft_tail<LOG2L, odd ? 1 : 2, LOW>(tw, b1, b0, last);
 }
@@ -291,7 +305,7 @@ __global__ void __launch_bounds__(kFftThreads) fdk_filter_kernel(const __grid_co
     constexpr bool odd = LOG2L & 1;
     extern __shared__ __align__(16) float2 fsm[];
     const int na = p.na;
-    float2 *b0 = fsm, *b1 = fsm + fpad(L), *tw = fsm + 2 * fpad(L);
+    float2 *b0 = fsm, *b1 = fsm + fft_buf(L), *tw = fsm + 2 * fft_buf(L);
     float *hs = reinterpret_cast<float *>(tw + L);
     // twiddle tables of the radix-4 stages: W^(r k L/(4 Ns)) = exp(-2 pi i r k / (4 Ns))
     for (int Ns = odd ? 2 : 1; Ns <= L / 4; Ns *= 4) {

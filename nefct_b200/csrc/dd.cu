@@ -13,7 +13,9 @@
 //    span of the bin's lower/upper z edges (:125-139);
 //  * every voxel inside both footprints gets value * (overlap fraction in v)
 //    * (overlap fraction in z) / |u21| * |p2 - p1| * SAD^2 / (SAD + x cos +
-//    y sin)^2 (:141-154).
+//    y sin)^2 (:141-154).  The footprints are evaluated with the reference's
+//    operations; the weights divide by multiplying with approximate
+//    reciprocals and group the per-column factors (a few ulp per weight).
 //
 // GPU structure (not the reference's): one warp walks 32 consecutive rows of
 // one detector column at one view.  The x and y parts of those rays are
@@ -125,7 +127,7 @@ __global__ void __launch_bounds__(256) dd_backproject_kernel(const __grid_consta
     const float hdb = __fdiv_rn(p.db, 2.f);
     const float rzl = __fdiv_rn(__fsub_rn(z21, hdb), u21), rzr = __fdiv_rn(__fadd_rn(z21, hdb), u21);
     const float vhalf = (float)(nvt / 2), zhalf = (float)(p.nz / 2), uhalf = __fdiv_rn((float)nu, 2.f);
-    const float au = dd_abs(u21);
+    const float len_au = __fdiv_rn(len, dd_abs(u21));
     const float sad2 = __fmul_rn(p.sad, p.sad);
     const float xhalf = (float)(p.nx / 2), yhalf = (float)(p.ny / 2);
     const unsigned zs = (unsigned)p.nz;
@@ -144,20 +146,24 @@ __global__ void __launch_bounds__(256) dd_backproject_kernel(const __grid_consta
         const float zi1 = dd_min(czl, czr), zi2 = dd_max(czl, czr);
         const int za = max(0, (int)floorf(zi1)), zb = live ? min(p.nz - 1, (int)floorf(zi2)) : -1;
         const float vspan = __fsub_rn(vi2, vi1), zspan = __fsub_rn(zi2, zi1);
+        // the reference's divisions by vspan, zspan and den become
+        // multiplications by approximate reciprocals (<= 1 ulp each)
+        const float ivspan = rcp_approx(vspan), izspan = rcp_approx(zspan);
         for (int iv2 = va; iv2 <= vb; ++iv2) {
-            const float wv = __fdiv_rn(__fsub_rn(dd_min((float)iv2 + 1.0f, vi2), dd_max((float)iv2, vi1)), vspan);
+            const float wv = __fmul_rn(__fsub_rn(dd_min((float)iv2 + 1.0f, vi2), dd_max((float)iv2, vi1)), ivspan);
             const int ix = xdrive ? iu : iv2, iy = xdrive ? iv2 : iu;
             // (ix + 0.5 - nx / 2): exact in float
             const float xc = __fsub_rn(__fadd_rn((float)ix, 0.5f), xhalf);
             const float yc = __fsub_rn(__fadd_rn((float)iy, 0.5f), yhalf);
             const float den = __fadd_rn(__fadd_rn(p.sad, __fmul_rn(xc, cphi)), __fmul_rn(yc, sphi));
-            const float fw = __fdiv_rn(__fdiv_rn(sad2, den), den);
+            const float iden = rcp_approx(den);
+            const float fw = __fmul_rn(__fmul_rn(sad2, iden), iden);
+            // value * wv * (len / |u21|) * fw per voxel of the column, times wz
+            const float cw = __fmul_rn(__fmul_rn(__fmul_rn(value, wv), len_au), fw);
             float *col = p.acc + ((size_t)iy * p.nx + ix) * zs;
             for (int iz = za; iz <= zb; ++iz) {
-                const float wz =
-                    __fdiv_rn(__fsub_rn(dd_min((float)iz + 1.0f, zi2), dd_max((float)iz, zi1)), zspan);
-                const float w = __fmul_rn(__fmul_rn(__fdiv_rn(__fmul_rn(wv, wz), au), len), fw);
-                atomicAdd(col + iz, __fmul_rn(value, w));
+                const float wz = __fmul_rn(__fsub_rn(dd_min((float)iz + 1.0f, zi2), dd_max((float)iz, zi1)), izspan);
+                atomicAdd(col + iz, __fmul_rn(cw, wz));
             }
         }
     }

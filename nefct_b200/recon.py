@@ -4,6 +4,12 @@
   backprojection (mat_codes/filtering.m + backprojection.m as one call);
 * ``sirt`` -- x <- x + lam * C A^T R (b - A x) with R, C the inverse row and
   column sums (the normalised form of nefct/functions/sart.py:29-39);
+* ``cg`` -- conjugate gradients on A^T A x = A^T b (the normal equations that
+  nefct/functions/conj_grad.py:76-101 iterates on), with its scalars kept on
+  the device;
+  both loops can run as one captured CUDA graph per iteration (``graph=True``):
+  the first iteration runs eagerly, the second is recorded and the rest are
+  replays, with no host synchronisation inside an iteration;
 * ``motion_project`` -- the 4D forward of project_t.py:153-160 with the
   cpp/deform warp: per phase, warp the reference volume by that phase's
   displacement field and project the phase's views; differentiable in the
@@ -17,15 +23,46 @@ import torch
 
 from . import _lib, ops
 
-__all__ = ["fdk", "sirt", "motion_project", "sinusoid_field"]
+__all__ = ["fdk", "sirt", "cg", "motion_project", "sinusoid_field"]
 
 
 def fdk(sino: torch.Tensor, geom: ops.ConeBeam, window: str = "ram-lak", parker: int = 0) -> torch.Tensor:
     return ops.fdk_backproject(ops.fdk_filter(sino, geom, window, parker), geom)
 
 
+def _iterate(step, n_iter: int, graph: bool, callback, state) -> None:
+    """Runs step() n_iter times; with graph=True the first call runs eagerly on
+    a side stream (its allocations warm the caching allocator), the second is
+    recorded into a CUDA graph and the remaining ones are replays of it."""
+    if n_iter <= 0:
+        return
+    if not graph:
+        for it in range(n_iter):
+            step()
+            if callback is not None:
+                callback(it, state)
+        return
+    side = torch.cuda.Stream(device=state.device)
+    side.wait_stream(torch.cuda.current_stream(state.device))
+    with torch.cuda.stream(side):
+        step()
+    torch.cuda.current_stream(state.device).wait_stream(side)
+    if callback is not None:
+        callback(0, state)
+    if n_iter == 1:
+        return
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        step()
+    for it in range(1, n_iter):
+        g.replay()
+        if callback is not None:
+            callback(it, state)
+    del g
+
+
 def sirt(b: torch.Tensor, geom: ops.ConeBeam, n_iter: int, flags: int = _lib.LINE_INTEGRAL, x0=None,
-         lam: float = 1.0, callback=None) -> torch.Tensor:
+         lam: float = 1.0, callback=None, graph: bool = False) -> torch.Tensor:
     ones_v = torch.ones(geom.vol_shape, device=b.device, dtype=b.dtype)
     ones_s = torch.ones(geom.sino_shape, device=b.device, dtype=b.dtype)
     rs = ops.cb_forward(ones_v, geom, flags)
@@ -36,13 +73,45 @@ def sirt(b: torch.Tensor, geom: ops.ConeBeam, n_iter: int, flags: int = _lib.LIN
     x = torch.zeros(geom.vol_shape, device=b.device, dtype=b.dtype) if x0 is None else x0.clone()
     ax = torch.empty_like(b)
     atr = torch.empty_like(x)
-    for it in range(n_iter):
+
+    def step():
         ops.cb_forward(x, geom, flags, out=ax)
         ax.sub_(b).neg_().mul_(R)                 # R (b - A x)
         ops.cb_backward(ax, geom, flags, out=atr)
         x.addcmul_(atr, C, value=lam)
-        if callback is not None:
-            callback(it, x)
+
+    _iterate(step, n_iter, graph, callback, x)
+    return x
+
+
+def cg(b: torch.Tensor, geom: ops.ConeBeam, n_iter: int, flags: int = _lib.LINE_INTEGRAL, x0=None,
+       callback=None, graph: bool = False) -> torch.Tensor:
+    """Conjugate gradients on A^T A x = A^T b; alpha and beta stay 0-dim
+    device tensors, so an iteration never waits for the host."""
+    ax = torch.empty_like(b)
+    aty = ops.cb_backward(b, geom, flags)
+    x = torch.zeros(geom.vol_shape, device=b.device, dtype=b.dtype) if x0 is None else x0.clone()
+    ata = torch.empty_like(x)
+
+    def normal(v):                                # A^T A v into ata
+        ops.cb_forward(v, geom, flags, out=ax)
+        ops.cb_backward(ax, geom, flags, out=ata)
+        return ata
+
+    r = aty - normal(x)
+    p = r.clone()
+    rsold = (r.double() * r.double()).sum()
+
+    def step():
+        ap = normal(p)
+        alpha = rsold / (p.double() * ap.double()).sum()
+        x.add_(p * alpha.float())
+        r.sub_(ap * alpha.float())
+        rsnew = (r.double() * r.double()).sum()
+        p.mul_((rsnew / rsold).float()).add_(r)
+        rsold.copy_(rsnew)
+
+    _iterate(step, n_iter, graph, callback, x)
     return x
 
 

@@ -109,6 +109,8 @@ def tune_cone_beam(geom: ops.ConeBeam, flags: int = 0, device=None, reps: int = 
                 wb = min(_WALKS, key=lambda w: t_dir[("bwd", w)])
                 for walk in _WALKS:
                     times[f"{rows}/{order}/{3 * walk}"] = t_dir[("fwd", walk)] + t_dir[("bwd", walk)]
+                    times[f"{rows}/{order}/{3 * walk}/fwd"] = t_dir[("fwd", walk)]
+                    times[f"{rows}/{order}/{3 * walk}/bwd"] = t_dir[("bwd", walk)]
                 total = t_dir[("fwd", wf)] + t_dir[("bwd", wb)]
                 if best is None or total < best[0]:
                     best = (total, rows, order, wf | (wb << 1))

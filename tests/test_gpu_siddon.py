@@ -232,16 +232,19 @@ def test_adjoint_512cube_720views_normal(cuda):
     torch.cuda.empty_cache()
 
 
-def test_launch_shapes_give_identical_forward(cuda):
+@pytest.mark.parametrize("size", [(40.0, 36.0, 30.0), (40.0, 46.8, 24.0)], ids=["cubic", "anisotropic"])
+def test_launch_shapes_give_identical_forward(cuda, size):
     """Launch shapes do not change the per-ray arithmetic: the forward is
     bitwise identical across rows (columns) per CTA, grid orders and the two
-    walks (thread per ray, column warps).  The geometry has a partial last row tile
-    (45 rows) and row tiles that straddle the central row (z slopes of both
-    signs in one warp); the transpose gets zero rays inside a warp.  The
-    transpose agrees to float rounding (atomic summation order)."""
+    walks (thread per ray, column warps), for cubic voxels and for voxels
+    of 1 x 1.3 x 0.8 mm (the walks' division path).  The geometry has a
+    partial last row tile (45 rows) and row tiles that straddle the central
+    row (z slopes of both signs in one warp); the transpose gets zero rays
+    inside a warp.  The transpose agrees to float rounding (atomic summation
+    order)."""
     from nefct_b200 import autotune
     g = nb.ConeBeam((40, 36, 30), np.linspace(0, 2 * np.pi, 33, endpoint=False), 150.0, 300.0, 70, 1.3, 45, 1.1,
-                    size=(40.0, 36.0, 30.0))
+                    size=size)
     gen = torch.Generator(device=cuda).manual_seed(8)
     vol = torch.rand(g.vol_shape, device=cuda, generator=gen)
     y = torch.rand(g.sino_shape, device=cuda, generator=gen)
@@ -264,7 +267,8 @@ def test_launch_shapes_give_identical_forward(cuda):
             assert float((b - backs[0]).norm() / backs[0].norm()) < 1e-6
         rec = autotune.tune_cone_beam(g, 0, cuda, reps=1, use_cache=False)
         assert rec["rows"] in (2, 4, 8) and rec["order"] in (0, 1) and rec["walk"] in (0, 1, 2, 3)
-        assert len(rec["ms"]) == 12
+        assert len([k for k in rec["ms"] if k.count("/") == 2]) == 12      # rows x order x walk, both directions
+        assert all(f"{k}/fwd" in rec["ms"] and f"{k}/bwd" in rec["ms"] for k in rec["ms"] if k.count("/") == 2)
     finally:
         autotune.apply(saved["rows"], saved["order"], saved["walk"])
 

@@ -100,14 +100,18 @@ def cg(b: torch.Tensor, geom: ops.ConeBeam, n_iter: int, flags: int = _lib.LINE_
 
     r = aty - normal(x)
     p = r.clone()
-    rsold = (r.double() * r.double()).sum()
+
+    def dot(u, v):                                # float32 products, float64 sum
+        return (u * v).sum(dtype=torch.float64)
+
+    rsold = dot(r, r)
 
     def step():
         ap = normal(p)
-        alpha = rsold / (p.double() * ap.double()).sum()
+        alpha = rsold / dot(p, ap)
         x.add_(p * alpha.float())
         r.sub_(ap * alpha.float())
-        rsnew = (r.double() * r.double()).sum()
+        rsnew = dot(r, r)
         p.mul_((rsnew / rsold).float()).add_(r)
         rsold.copy_(rsnew)
 

@@ -221,8 +221,14 @@ __global__ void __launch_bounds__(256) lor_key_kernel(const __grid_constant__ Lo
             const float f = fminf(fmaxf((v - lo) / (hi - lo), 0.f), 1.f);
             return (unsigned)fminf(f * (float)(1 << bits), (float)((1 << bits) - 1));
         };
-        const unsigned k = (xdrive << 30) | (q(th, 0.f, 3.14159265f, 8) << 22) | (q(perp, -1.f, 1.f, 8) << 14) |
-                           (q(zc, -1.f, 1.f, 7) << 7) | q(atanf(slope), -1.5708f, 1.5708f, 7);
+        // z centre and slope interleaved bit by bit (a Z-order curve): the
+        // lines of one direction and offset bin fall into warps of similar
+        // z entry and exit, so the walks of a warp have similar lengths
+        const unsigned zq = q(zc, -1.f, 1.f, 7), sq = q(atanf(slope), -1.5708f, 1.5708f, 7);
+        unsigned zs = 0;
+#pragma unroll
+        for (int b = 0; b < 7; ++b) zs |= ((zq >> b) & 1u) << (2 * b + 1) | ((sq >> b) & 1u) << (2 * b);
+        const unsigned k = (xdrive << 30) | (q(th, 0.f, 3.14159265f, 8) << 22) | (q(perp, -1.f, 1.f, 8) << 14) | zs;
         keys[i] = (int32_t)k;
     }
 }

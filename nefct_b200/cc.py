@@ -99,16 +99,33 @@ def _pixel_backproject(cyl):
     return op
 
 
+# Line lists at least this long are walked in lor_order (a key pass and a
+# sort, ~1 ms for 16 Mi lines, against a 6-8x slower walk in list order); the
+# results keep the lines' order, so the ops behave exactly as in list order
+# (the backprojection up to the summation order of its float reductions).
+_LOR_AUTO_ORDER = 1 << 20
+
+
+def _lor_walk_order(lors, g, center, size):
+    if lors.shape[1] < _LOR_AUTO_ORDER:
+        return None
+    return ops.lor_order(lors, g, center, size)
+
+
 def _projection(lors, image, grid, center, size):
     g = _host3(grid, int)
-    return ops.lor_forward(lors.contiguous(), _flat_volume(image, g), g, _host3(center, float),
-                           _host3(size, float), _lib.LOR_REF_FORWARD)
+    lors = lors.contiguous()
+    c, s = _host3(center, float), _host3(size, float)
+    return ops.lor_forward(lors, _flat_volume(image, g), g, c, s, _lib.LOR_REF_FORWARD,
+                           order=_lor_walk_order(lors, g, c, s))
 
 
 def _backprojection(image, lors, lors_value, grid, center, size):
     g = _host3(grid, int)
-    vol = ops.lor_backward(lors.contiguous(), lors_value.contiguous(), g, _host3(center, float),
-                           _host3(size, float), _lib.LOR_REF_BACKPROJECT)
+    lors = lors.contiguous()
+    c, s = _host3(center, float), _host3(size, float)
+    vol = ops.lor_backward(lors, lors_value.contiguous(), g, c, s, _lib.LOR_REF_BACKPROJECT,
+                           order=_lor_walk_order(lors, g, c, s))
     return vol.view(image.shape)
 
 

@@ -99,3 +99,24 @@ def test_op_mirrors_reproduce_quirks(cuda, golden):
     g = nb.ConeBeam((24, 20, 16), golden["angles"], SRC_ISO, SRC_DET, NA, 2.5, NB, 2.5, AI, BI,
                     (1.0, -0.5, 0.25), (48.0, 40.0, 32.0))
     np.testing.assert_array_equal(a.cpu().numpy(), ops.cb_forward(vol, g).cpu().numpy())
+
+
+def test_lor_op_mirrors_order_long_lists(cuda):
+    """The Projection / Backprojection mirrors walk lists of >= 2^20 lines in
+    lor_order: the forward equals the list-order walk bit for bit, the
+    backprojection to float rounding (summation order of the reductions)."""
+    n, shape, size = (1 << 20) + 4097, (32, 28, 24), (64.0, 56.0, 48.0)
+    gen = torch.Generator(device=cuda).manual_seed(12)
+    ang = torch.rand(2, n, device=cuda, generator=gen) * (2 * np.pi)
+    zz = (torch.rand(2, n, device=cuda, generator=gen) - 0.5) * 60.0
+    lors = torch.stack([50.0 * torch.cos(ang[0]), 50.0 * torch.sin(ang[0]), zz[0],
+                        50.0 * torch.cos(ang[1]), 50.0 * torch.sin(ang[1]), zz[1]]).contiguous()
+    image = torch.rand(shape, device=cuda, generator=gen)          # [nx, ny, nz] of the TF op
+    vals = torch.rand(n, device=cuda, generator=gen)
+    center = (0.0, 0.0, 0.0)
+    a = nb.cc.siddon.projection(lors, image, shape, center, size)
+    a0 = ops.lor_forward(lors, image.contiguous().view(24, 28, 32), shape, center, size, _lib.LOR_REF_FORWARD)
+    assert torch.equal(a, a0)
+    b = nb.cc.siddon.backprojection(image, lors, vals, shape, center, size).double()
+    b0 = ops.lor_backward(lors, vals, shape, center, size, _lib.LOR_REF_BACKPROJECT).view(image.shape).double()
+    assert float((b - b0).norm() / b0.norm()) < 1e-6

@@ -387,14 +387,14 @@ static cudaError_t launch_filter(const FilterParams &p, const float *sino, float
 #endif
 static constexpr int kZ = NEFCT_FDK_KZ; // voxels along z per thread
 // Views per launch: as many as keep a chunk of filtered projections within
-// ~38 MB (an L2-resident chunk beside an L2-resident 256^3 volume), 8 to 64
-// (48 for 512 x 384 detectors; measured 2 % faster than 32 and 7 % than 16,
-// fewer read-modify-write passes over the volume).
+// ~52 MB (an L2-resident chunk beside an L2-resident 256^3 volume), 8 to 64
+// (64 for 512 x 384 detectors; measured 1 % faster than 48, 3 % than 32 and
+// 8 % than 16: fewer read-modify-write passes over the volume).
 static constexpr int kViewChunk = 64;
 static inline int fdk_view_chunk(int na, int nb)
 {
     const double per_view = (double)na * nb * sizeof(float);
-    return (int)std::min<double>(kViewChunk, std::max<double>(8.0, (double)(38 << 20) / per_view));
+    return (int)std::min<double>(kViewChunk, std::max<double>(8.0, (double)(52 << 20) / per_view));
 }
 // A warp owns an 8 x 4 (x, y) tile of voxel columns: at any view its
 // voxels project onto fewer detector columns than a 32 x 1 row (whose

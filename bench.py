@@ -360,6 +360,22 @@ def run_gpu(args):
         fdk[win] = {"filter_ms": 1e3 * t_f, "backproject_ms": 1e3 * t_b,
                     "voxels_per_s": n ** 3 / (t_f + t_b), "voxel_views_per_s": n ** 3 * CFG["nv"] / t_b,
                     "central_rel_error_vs_phantom": err}
+    # the reference's voxel-driven backprojection (pixel_3d: the FDK body
+    # without its distance weight) built for the host, on a 2-view sample
+    # scaled to the scan, beside the GPU backprojection of all views
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        import oracle
+        if oracle.have_ref():
+            hs = filt[:2].cpu().numpy()
+            side = n * CFG["voxel"]
+            t0 = time.perf_counter()
+            oracle.ref_pixel_backproject(hs, angles()[:2], (n, n, n), (-side / 2,) * 3, (side,) * 3,
+                                         CFG["src_iso"], CFG["src_det"], CFG["na"], CFG["pixel"], 0.0,
+                                         CFG["nb"], CFG["pixel"], 0.0)
+            t_host = (time.perf_counter() - t0) * CFG["nv"] / 2
+            fdk["reference_host_build"] = {"cores": os.cpu_count(), "sample": "2 views, scaled to the scan",
+                                           "pixel_backproject_ms": 1e3 * t_host,
+                                           "speedup_of_fdk_backproject": t_host / t_b}
     # short scan 180 deg + fan with Parker weights (views spaced like the full scan)
     fan = 2 * np.degrees(np.arctan(CFG["na"] * CFG["pixel"] / 2 / CFG["src_det"]))
     step = 360.0 / CFG["nv"]

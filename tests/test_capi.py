@@ -97,3 +97,41 @@ def test_deterministic_workspace_size(nefct_lib):
     n = 16 ** 3
     assert nefct_lib.nefct_cb_workspace_bytes(C.byref(g), 0x40) == 256 + 16 * n
     assert nefct_lib.nefct_cb_workspace_bytes(C.byref(g), 0x40 | 0x20) == 256 + 8 * n
+
+
+def test_fdk_filter_rejects_wide_detectors(nefct_lib):
+    """The filter's transforms go up to 4096 points: more than 2048 columns is
+    refused before any device work."""
+    g = _geom(na=2049).struct()
+    assert nefct_lib.nefct_fdk_filter(C.byref(g), C.c_void_p(16), C.c_void_p(32), 0, 0, None) == 5
+    assert b"2048" in nefct_lib.nefct_last_error()
+
+
+def test_batch_plan_validates_problems(nefct_lib):
+    from nefct_b200 import _lib
+    probs = (_lib.CBProblem * 97)()
+    plan, ws = C.c_void_p(), C.c_size_t()
+    assert nefct_lib.nefct_cb_batch_plan(probs, 97, 0, C.byref(plan), C.byref(ws)) == 1   # > 96 problems
+    assert b"96" in nefct_lib.nefct_last_error()
+    probs = (_lib.CBProblem * 1)()
+    probs[0].geom = _geom().struct()
+    assert nefct_lib.nefct_cb_batch_plan(probs, 1, 0, C.byref(plan), C.byref(ws)) == 1     # NULL buffers
+    assert b"NULL" in nefct_lib.nefct_last_error()
+    probs[0].vol = probs[0].sino = probs[0].grad = probs[0].back = 16
+    assert nefct_lib.nefct_cb_batch_plan(probs, 1, 0x4000, C.byref(plan), C.byref(ws)) == 1  # unknown flags
+
+
+def test_dd_rejects_bad_geometry(nefct_lib):
+    from nefct_b200 import _lib
+    ang = (C.c_float * 2)(0.0, float("nan"))
+    g = _lib.DDGeom(nx=8, ny=8, nz=8, nv=2, angles=ang, z_offsets=None, src_iso=100.0, src_det=200.0, na=16,
+                    da=1.0, a_offset=0.0, nb=8, db=1.0, b_offset=0.0, det_kind=0)
+    ws = nefct_lib.nefct_dd_workspace_bytes(C.byref(g))
+    assert ws == 8 * 8 * 8 * 4
+    assert nefct_lib.nefct_dd_backproject(C.byref(g), C.c_void_p(16), C.c_void_p(32), C.c_void_p(64), ws, None) == 1
+    assert b"view 1" in nefct_lib.nefct_last_error()
+    ang[1] = 0.5
+    g.det_kind = 7
+    assert nefct_lib.nefct_dd_backproject(C.byref(g), C.c_void_p(16), C.c_void_p(32), C.c_void_p(64), ws, None) == 1
+    g.det_kind = 0
+    assert nefct_lib.nefct_dd_backproject(C.byref(g), C.c_void_p(16), C.c_void_p(32), C.c_void_p(64), 4, None) == 3

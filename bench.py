@@ -418,9 +418,10 @@ def run_gpu(args):
 
 # ---------------- batched uneven problems (64 problems, edges 64..384) ----------------
 
-def uneven_geoms(n_problems=64, seed=4, scale=1.0):
+def uneven_geoms(n_problems=64, seed=4, scale=1.0, view_scale=1.0):
     """Seeded uneven problems: edge log-uniform in [64, 384] (times scale),
-    views U{60..720}, detector rows/cols U{128..1024} (times scale), source-axis
+    views U{60..720} (times view_scale, at least 4), detector rows/cols
+    U{128..1024} (times scale), source-axis
     U[400, 700] mm, source-detector = source-axis x U[1.5, 2.0], 1 mm voxels,
     square pixels sized so the detector width covers the volume."""
     import nefct_b200 as nb
@@ -428,7 +429,7 @@ def uneven_geoms(n_problems=64, seed=4, scale=1.0):
     geoms = []
     for _ in range(n_problems):
         n = int(round(np.exp(rng.uniform(np.log(64), np.log(384))) * scale))
-        nv = int(rng.integers(60, 721))
+        nv = max(4, int(round(int(rng.integers(60, 721)) * view_scale)))
         rows, cols = (int(round(v * scale)) for v in rng.integers(128, 1025, 2))
         si = float(rng.uniform(400, 700))
         sd = si * float(rng.uniform(1.5, 2.0))
@@ -448,7 +449,7 @@ def run_batched(args):
     from nefct_b200.batch import BatchProjector
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    geoms = uneven_geoms(args.problems, 4, args.scale)
+    geoms = uneven_geoms(args.problems, 4, args.scale, args.view_scale)
     gen = torch.Generator(device=dev).manual_seed(4)
     vols = [torch.rand(g.vol_shape, device=dev, generator=gen) for g in geoms]
     bp = BatchProjector(geoms, vols)            # grads = the forward outputs (loss = |Ax|^2 / 2)
@@ -493,7 +494,8 @@ def run_batched(args):
             "unit": "iterations/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * t_batch, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded uniform random volumes)",
-            "config": {"workload": f"{args.problems} problems, edge log-U[64,384]x{args.scale}, views U[60,720], "
+            "config": {"workload": f"{args.problems} problems, edge log-U[64,384]x{args.scale}, "
+                                   f"views U[60,720]x{args.view_scale}, "
                                    f"detector U[128,1024]^2 x{args.scale}, seed 4",
                        "voxels": int(sum(np.prod(g.shape) for g in geoms)),
                        "rays": int(sum(g.nv * g.na * g.nb for g in geoms)), "tiles": bp.tiles},
@@ -749,6 +751,7 @@ def main():
                     help="batched: the 64 uneven problems (its own JSON line)")
     ap.add_argument("--problems", type=int, default=64)
     ap.add_argument("--scale", type=float, default=1.0, help="batched: scale of volume edges and detector sizes")
+    ap.add_argument("--view-scale", type=float, default=1.0, help="batched: scale of the view counts")
     args = ap.parse_args()
     CFG["nv"] = args.views
     if args.impl == "reference":

@@ -21,5 +21,6 @@ from .ops import ConeBeam, backproject, project, warp
 from .functions import (FDK, SART, BackProject3D, BackProject3DT, ConjGrad, Project3D, Project3DT,
                         WarpDeformer, cone_beam)
 from . import cc
+from . import recon
 
 __version__ = "0.1.0"

@@ -335,6 +335,21 @@ size_t nefct_dd_workspace_bytes(const nefct_dd_geom *g);
 nefct_status nefct_dd_backproject(const nefct_dd_geom *g, const float *proj, float *vol, void *ws, size_t ws_bytes,
                                   void *stream);
 
+/* ---- ceiling probes (measurement; no counterpart in the reference) ----
+ * The cone-beam walks read and reduce mostly L2-resident data, so their
+ * rooflines are set by the L2 read bandwidth and the L2 reduction rate of
+ * the GPU at hand.  nefct_probe_l2_read streams n floats of buf (16-byte
+ * aligned, n a multiple of 4; size it to stay in L2) `reps` times with
+ * 16-byte L2-only loads; nefct_probe_l2_red adds 1.0f to each of n floats of
+ * buf `reps` times with coalesced red.global.add.f32.  Both run
+ * blocks_per_sm x (SM count) CTAs of 256 threads; sink takes
+ * nefct_probe_sink_floats(blocks_per_sm) floats.  Time them with events on
+ * `stream`. */
+size_t nefct_probe_sink_floats(int32_t blocks_per_sm);
+nefct_status nefct_probe_l2_read(const float *buf, size_t n, int32_t reps, int32_t blocks_per_sm, float *sink,
+                                 void *stream);
+nefct_status nefct_probe_l2_red(float *buf, size_t n, int32_t reps, int32_t blocks_per_sm, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -129,8 +129,9 @@ class ProjectionSequence3D(_ArithmeticMixin):
 # ---------------- phantoms ----------------
 
 def _rotation(phi, theta, psi):
-    """Euler rotation of nefct/data/sl_phantom.py:130-139 (degrees in)."""
-    phi, theta, psi = (np.deg2rad(v) for v in (phi, theta, psi))
+    """Euler rotation of nefct/data/sl_phantom.py:130-139 (degrees in,
+    converted as there: v * pi / 180)."""
+    phi, theta, psi = (v * np.pi / 180 for v in (phi, theta, psi))
     cphi, sphi, cth, sth, cpsi, spsi = np.cos(phi), np.sin(phi), np.cos(theta), np.sin(theta), np.cos(psi), np.sin(psi)
     return np.array([[cpsi * cphi - cth * sphi * spsi, cpsi * sphi + cth * cphi * spsi, spsi * sth],
                      [-spsi * cphi - cth * sphi * cpsi, -spsi * sphi + cth * cphi * cpsi, cpsi * sth],
@@ -142,24 +143,41 @@ def ellipsoid_phantom(n, ellipsoids, device=None, dtype=torch.float32) -> torch.
 
     Rows are [A, a, b, c, x0, y0, z0, phi, theta, psi] in the [-1, 1]^3 box;
     grid coordinates linspace(-1 + 2/n, 1 - 2/n, n) (sl_phantom.py:109-148).
-    Evaluated in float64 with torch on ``device`` (a GPU makes 512^3 cheap).
+    Evaluated in float64 with torch on ``device``.  Each ellipsoid is tested
+    only on the grid points of its bounding box (widened by two points):
+    the per-point arithmetic is the full-grid test's, and points outside the
+    box fail it, so the sum is the same to the bit.
     """
     if np.isscalar(n):
         n = (int(n),) * 3
     dev = torch.device(device) if device is not None else torch.device("cpu")
-    rng = [torch.linspace(-1 + 2 / k, 1 - 2 / k, k, dtype=torch.float64, device=dev) for k in n]
+    # numpy's linspace (the reference's grid, sl_phantom.py:114) to the bit
+    rng = [torch.from_numpy(np.linspace(-1 + 2 / k, 1 - 2 / k, k)).to(dev) for k in n]
     p = torch.zeros(n, dtype=torch.float64, device=dev)
-    xg = rng[0].view(-1, 1, 1)
-    yg = rng[1].view(1, -1, 1)
-    zg = rng[2].view(1, 1, -1)
     for e in ellipsoids:
         A, a, b, c, x0, y0, z0, phi, theta, psi = [float(v) for v in e]
         al = _rotation(phi, theta, psi)
+        # grid point q lies inside when u = al^T q is inside the axis-aligned
+        # ellipsoid at (x0, y0, z0); q = al u spans centre +- half along each axis
+        centre = al @ np.array([x0, y0, z0])
+        half = np.sqrt((al * np.array([a, b, c])) ** 2 @ np.ones(3))
+        box = []
+        for ax in range(3):
+            k = n[ax]
+            step = (2 - 4 / k) / (k - 1) if k > 1 else 1.0
+            lo = int(np.floor((centre[ax] - half[ax] - (-1 + 2 / k)) / step)) - 2
+            hi = int(np.ceil((centre[ax] + half[ax] - (-1 + 2 / k)) / step)) + 3
+            box.append(slice(max(lo, 0), min(hi, k)))
+        if any(s.start >= s.stop for s in box):
+            continue
+        xg = rng[0][box[0]].view(-1, 1, 1)
+        yg = rng[1][box[1]].view(1, -1, 1)
+        zg = rng[2][box[2]].view(1, 1, -1)
         x = xg * al[0, 0] + yg * al[1, 0] + zg * al[2, 0]
         y = xg * al[0, 1] + yg * al[1, 1] + zg * al[2, 1]
         z = xg * al[0, 2] + yg * al[1, 2] + zg * al[2, 2]
         idx = (x - x0) ** 2 / a ** 2 + (y - y0) ** 2 / b ** 2 + (z - z0) ** 2 / c ** 2 <= 1
-        p += A * idx
+        p[box[0], box[1], box[2]] += idx.to(torch.float64) * A      # A in float64, as p[idx] += A
     return p.to(dtype)
 
 

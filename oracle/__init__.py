@@ -43,11 +43,12 @@ class Grid(C.Structure):
 
 
 def build(ref: str | None = None) -> None:
-    """Run oracle/Makefile (C restatement, plus oracle/_ref when the
-    reference checkout is present)."""
+    """Run oracle/Makefile: the C restatement, plus oracle/_ref when a
+    reference checkout is named (``ref``, else the NEFCT_REF environment
+    variable)."""
     env = dict(os.environ)
     if ref:
-        env["REF"] = ref
+        env["NEFCT_REF"] = ref
     subprocess.run(["make", "-s", "-C", HERE], check=True, env=env)
 
 
@@ -66,6 +67,12 @@ def lib() -> C.CDLL:
 
 def have_ref() -> bool:
     return os.path.exists(_REF)
+
+
+def ref_threads() -> int:
+    """OpenMP threads the reference build runs on (OMP_NUM_THREADS, else
+    every host core)."""
+    return int(ref().ref_max_threads())
 
 
 def ref() -> C.CDLL:
@@ -264,13 +271,20 @@ def ref_cb_forward(g: Grid, vol, angles, SID, SAD, na, da, ai, nb, db, bi, *, cy
     return out
 
 
-def ref_cb_backward(g: Grid, sino, angles, SID, SAD, na, da, ai, nb, db, bi, *, cyl=False, f64=False):
+def ref_cb_backward(g: Grid, sino, angles, SID, SAD, na, da, ai, nb, db, bi, *, cyl=False, f64=False,
+                    atomic=False):
+    """The reference's backprojection.  Default: deterministic (fixed chunks
+    of rows, chunk volumes summed in order; 16 volume-sized buffers).
+    atomic=True: atomic adds into one volume (the host form of the device
+    atomics: no extra volumes, summation order set by scheduling) -- for
+    timing and for volumes too large for 16 copies."""
     R = ref()
     nv = len(angles)
     if f64:
         conv, cv, fn, dt = _f64, C.c_double, R.ref_s3d_backproject_f64, np.float64
     else:
-        conv, cv, fn, dt = _f32, C.c_float, R.ref_s3d_backproject, np.float32
+        conv, cv, dt = _f32, C.c_float, np.float32
+        fn = R.ref_s3d_backproject_atomic if atomic else R.ref_s3d_backproject
     s = conv(sino).reshape(-1)
     if cyl:
         # Q8 indexing reaches ia + iv*na + ib*na*nb; pad with zeros past the end

@@ -14,6 +14,10 @@
 #endif
 #include "nefct_oracle.h"
 
+/* Deterministic scatters split their rows into this many chunks, whatever the
+ * thread count (the reference build's shim uses the same number). */
+#define OR_CHUNKS 16
+
 /* ---- slab walk, cone-beam and LOR drivers: float and double builds ---- */
 #define REAL float
 #define SUF _f32
@@ -293,9 +297,9 @@ void or_warp_invert_f32(const float *mx, const float *my, const float *mz, int n
  * (or |y21|) * |p2 - p1| * SAD^2 / (SAD + x cos + y sin)^2 (:148-154).
  * Voxel units, grid centred on the axis, SID = source-detector and SAD =
  * source-axis (the python naming used there).  The float/double promotions
- * of the reference expressions are spelled out.  Views are split across
- * OpenMP threads with private volumes summed in thread order, as in the
- * reference build's shim, so the two agree bit for bit. */
+ * of the reference expressions are spelled out.  The (view, row) pairs form
+ * OR_CHUNKS fixed chunks with private volumes summed in chunk order, as in
+ * the reference build's shim, so the two agree bit for bit. */
 #define DD_ABS(x) (((x) > 0) ? (x) : -(x))
 #define DD_MIN(a, b) (((a) < (b)) ? (a) : (b))
 #define DD_MAX(a, b) (((a) > (b)) ? (a) : (b))
@@ -389,22 +393,22 @@ void or_dd_backproject_f32(const float *proj, const float *cs, const float *sn, 
                            float SID, float SAD, int nx, int ny, int nz, int na, float da, float ai, int nb,
                            float db, float bi, int cyl, int use_cosf, float *img)
 {
-    const long long nvox = (long long)nx * ny * nz;
-    const int nth = omp_get_max_threads();
-    float *priv = (float *)calloc((size_t)nth * nvox, sizeof(float));
-    #pragma omp parallel
-    {
-        float *mine = priv + (long long)omp_get_thread_num() * nvox;
-        #pragma omp for schedule(static)
-        for (int iv = 0; iv < nv; ++iv)
-            for (int ib = 0; ib < nb; ++ib)
-                for (int ia = 0; ia < na; ++ia)
-                    dd_bin(cyl, cs, sn, off, SID, SAD, nx, ny, nz, da, ai, na, db, bi, nb, ia, ib, iv, use_cosf,
-                           proj[ia + (long long)ib * na + (long long)iv * na * nb], mine);
+    const long long nvox = (long long)nx * ny * nz, rows = (long long)nv * nb;
+    float *priv = (float *)calloc((size_t)OR_CHUNKS * nvox, sizeof(float));
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int c = 0; c < OR_CHUNKS; ++c) {
+        float *mine = priv + (long long)c * nvox;
+        for (long long r = rows * c / OR_CHUNKS; r < rows * (c + 1) / OR_CHUNKS; ++r) {
+            const int iv = (int)(r / nb), ib = (int)(r % nb);
+            for (int ia = 0; ia < na; ++ia)
+                dd_bin(cyl, cs, sn, off, SID, SAD, nx, ny, nz, da, ai, na, db, bi, nb, ia, ib, iv, use_cosf,
+                       proj[ia + (long long)ib * na + (long long)iv * na * nb], mine);
+        }
     }
+    #pragma omp parallel for schedule(static)
     for (long long i = 0; i < nvox; ++i) {
         float s = 0.0f;
-        for (int t = 0; t < nth; ++t) s += priv[(long long)t * nvox + i];
+        for (int c = 0; c < OR_CHUNKS; ++c) s += priv[(long long)c * nvox + i];
         img[i] = s;
     }
     free(priv);

@@ -1,12 +1,14 @@
 """Benchmark: cone-beam forward projection + exact adjoint on one B200.
 
-Workload (default, the FDK scanner): 256^3 float32 volume of
-1 mm voxels holding 30 seeded ellipsoids, 360 views over 360 deg, flat
-detector 512 x 384 at 1.2 mm, source-axis 600 mm, source-detector 1200 mm.
-One step = forward projection (reference slab-split weights) of the volume
-plus the exact transpose applied to a dense incoming gradient sinogram (what
-one autograd forward+backward of the projector does; a dense gradient has no
-zero rays for the adjoint to skip).
+Headline workload (the differentiable-projector scan, the largest that runs
+on one GPU): 512^3 float32 volume of 1 mm voxels holding 50 seeded
+ellipsoids, 720 views over 360 deg, flat detector 1024 x 768 at 1 mm,
+source-axis 700 mm, source-detector 1400 mm.  One step = forward projection
+(reference slab-split weights) of the volume plus the exact transpose applied
+to a dense incoming gradient sinogram (what one autograd forward+backward of
+the projector does; a dense gradient has no zero rays for the adjoint to
+skip).  ``--workload fdk-scanner`` runs the same step on the FDK scanner
+(256^3 at 1 mm, 30 ellipsoids, 360 views, 512 x 384 at 1.2 mm, 600 / 1200 mm).
 
 Metric: ray-voxel intersections per second, forward + adjoint (I
 intersections each, I counted exactly by the count kernel).
@@ -16,6 +18,11 @@ intersections each, I counted exactly by the count kernel).
 N > 1: launched by torchrun, one rank per GPU; every rank runs its own scan
 (independent seeded phantom), no collective on the data path ("weak").
 Rank 0 prints one JSON line.
+
+--impl reference: the reference's own projector code (siddon_3d forward and
+backprojection device routines compiled for the host, oracle/_ref) on a
+sample of the same scan's views, on every host core; same metric and
+config.
 """
 from __future__ import annotations
 
@@ -32,28 +39,34 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-CFG = dict(n=256, voxel=1.0, ellipsoids=30, seed=2, nv=360, na=512, nb=384, pixel=1.2,
-           src_iso=600.0, src_det=1200.0)
+SCANS = {
+    "diff-projector": dict(n=512, voxel=1.0, ellipsoids=50, seed=3, nv=720, na=1024, nb=768, pixel=1.0,
+                           src_iso=700.0, src_det=1400.0, tune_every=6),
+    "fdk-scanner": dict(n=256, voxel=1.0, ellipsoids=30, seed=2, nv=360, na=512, nb=384, pixel=1.2,
+                        src_iso=600.0, src_det=1200.0, tune_every=1),
+}
 METRIC = "ray-voxel intersections/s (forward + adjoint)"
 UNIT = "intersections/s"
+CPU_VIEWS_PER_STEP = 2        # views of the reference's host build per sampled step
 
 
-def workload_name(c=CFG):
-    return (f"cone-beam fwd+adjoint {c['n']}^3 @{c['voxel']}mm, {c['ellipsoids']} ellipsoids, {c['nv']} views, "
-            f"{c['na']}x{c['nb']} @{c['pixel']}mm, SID {c['src_iso']:.0f} / SDD {c['src_det']:.0f} mm")
+def workload_name(c):
+    return (f"cone-beam fwd+adjoint {c['n']}^3 @{c['voxel']}mm, {c['ellipsoids']} ellipsoids (seed {c['seed']}), "
+            f"{c['nv']} views, {c['na']}x{c['nb']} @{c['pixel']}mm, SID {c['src_iso']:.0f} / SDD "
+            f"{c['src_det']:.0f} mm")
 
 
-def config_dict(extra=None):
-    d = {"workload": workload_name(), "volume": [CFG["n"]] * 3, "views": CFG["nv"],
-         "detector": [CFG["na"], CFG["nb"]], "l2": "flushed between timed steps (256 MiB write)",
-         "parallelism": "independent scan per GPU"}
-    if extra:
-        d.update(extra)
-    return d
+def config_dict(c):
+    """The config both arms print (identical dicts)."""
+    return {"workload": workload_name(c), "volume": [c["n"]] * 3, "views": c["nv"],
+            "detector": [c["na"], c["nb"]],
+            "l2": "inputs larger than L2; 256 MiB L2 flush between timed steps" if c["n"] >= 512
+            else "256 MiB L2 flush between timed steps",
+            "parallelism": "independent scan per GPU"}
 
 
-def angles():
-    return np.linspace(0, 2 * np.pi, CFG["nv"], endpoint=False).astype(np.float32)
+def angles(c):
+    return np.linspace(0, 2 * np.pi, c["nv"], endpoint=False).astype(np.float32)
 
 
 def load_peaks():
@@ -65,12 +78,13 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def load_traffic():
-    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary."""
+def load_traffic(workload):
+    """Per-launch DRAM bytes of each kernel of a workload, from the committed
+    ncu summary (profiles/traffic.json)."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(p):
         with open(p) as f:
-            return json.load(f)
+            return json.load(f).get(workload, {})
     return {}
 
 
@@ -121,7 +135,7 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def dist_setup(n_gpus):
+def dist_setup():
     import torch
     import torch.distributed as dist
     ws = int(os.environ.get("WORLD_SIZE", "1"))
@@ -152,59 +166,130 @@ def barrier(ws):
     torch.cuda.synchronize()
 
 
-# ---------------- CPU baseline (the reference, compiled for the host) ----------------
+# ---------------- the reference's host build on sampled views ----------------
 
-def cpu_sample(views_per_step, steps, warmup=0, seed=2):
-    """Times the reference's own forward + backprojection (oracle/_ref, or the
-    oracle restatement when the reference build is absent) on a subset of
-    views of the workload, all host threads.  Returns (I/s, kind, cores, sample)."""
-    import oracle
+def phantom_xfast(c, device=None):
+    """The scan's phantom as a [z][y][x] float32 array (torch on ``device``)."""
     import nefct_b200 as nb
-    import torch
-    kind = "reference" if oracle.have_ref() else "port"
-    n = CFG["n"]
-    vol = nb.ellipsoid_phantom(n, nb.random_ellipsoids(CFG["ellipsoids"], seed),
-                               device="cuda" if torch.cuda.is_available() else None)
-    vol = vol.permute(2, 1, 0).contiguous().cpu().numpy()
-    g = oracle.grid((n, n, n), (0, 0, 0), (n * CFG["voxel"],) * 3)
-    ang = angles()
-    a = (CFG["src_iso"], CFG["src_det"], CFG["na"], CFG["pixel"], 0.5, CFG["nb"], CFG["pixel"], 0.5)
-    tot_i, tot_t = 0, 0.0
-    for s in range(warmup + steps):
-        idx = [(s * views_per_step + k) * 37 % CFG["nv"] for k in range(views_per_step)]
-        sub = ang[idx]
-        _, cnt = oracle.cb_forward(g, vol, sub, *a)        # exact count of the sample
+    vol = nb.ellipsoid_phantom(c["n"], nb.random_ellipsoids(c["ellipsoids"], c["seed"]), device=device)
+    return vol.permute(2, 1, 0).contiguous()
+
+
+def sample_views(c, step, pairs=8):
+    """Views of sampled step `step`: CPU_VIEWS_PER_STEP views spread over the
+    scan, cycling through `pairs` fixed sets (so their exact intersection
+    counts are computed once)."""
+    s = step % pairs
+    return [((s * CPU_VIEWS_PER_STEP + k) * 97 + 13 * s) % c["nv"] for k in range(CPU_VIEWS_PER_STEP)]
+
+
+class HostReference:
+    """The reference's forward (ProjectFlatKernel) and backprojection
+    (BackProjectFlatKernel, atomic adds) built for the host (oracle/_ref; the
+    oracle restatement if the build is absent), over (view, row) pairs on
+    every host thread.  Intersections are counted exactly by the oracle's
+    walk, once per view set."""
+
+    def __init__(self, c, vol_np):
+        import oracle
+        self.o = oracle
+        self.c = c
+        self.kind = "reference" if oracle.have_ref() else "port"
+        n = c["n"]
+        self.g = oracle.grid((n, n, n), (0, 0, 0), (n * c["voxel"],) * 3)
+        self.vol = vol_np
+        self.ang = angles(c)
+        self.args = (c["src_iso"], c["src_det"], c["na"], c["pixel"], 0.5, c["nb"], c["pixel"], 0.5)
+        self.counts = {}
+
+    def threads(self):
+        return self.o.ref_threads() if self.kind == "reference" else (os.cpu_count() or 1)
+
+    def count(self, idx):
+        key = tuple(idx)
+        if key not in self.counts:
+            _, cnt = self.o.cb_forward(self.g, self.vol, self.ang[idx], *self.args)
+            self.counts[key] = cnt
+        return self.counts[key]
+
+    def step(self, idx):
+        """(seconds, forward sinogram, backprojection) of the views idx."""
+        sub = self.ang[idx]
         t0 = time.perf_counter()
-        if kind == "reference":
-            sino = oracle.ref_cb_forward(g, vol, sub, *a)
-            oracle.ref_cb_backward(g, sino, sub, *a)
+        if self.kind == "reference":
+            sino = self.o.ref_cb_forward(self.g, self.vol, sub, *self.args)
+            back = self.o.ref_cb_backward(self.g, sino, sub, *self.args, atomic=True)
         else:
-            sino, _ = oracle.cb_forward(g, vol, sub, *a, use_cosf=True)
-            oracle.cb_backward(g, sino, sub, *a, use_cosf=True)
-        dt = time.perf_counter() - t0
-        if s >= warmup:
-            tot_i += 2 * cnt
-            tot_t += dt
-    cores = os.cpu_count() or 1
-    sample = (f"{views_per_step} views per step ({steps} steps) of the workload: reference siddon_3d "
-              f"project_flat + backproject_flat device code compiled as host C++ (-O3, OpenMP)")
-    return tot_i / tot_t, kind, cores, sample
+            sino, _ = self.o.cb_forward(self.g, self.vol, sub, *self.args, use_cosf=True)
+            back = self.o.cb_backward(self.g, sino, sub, *self.args, use_cosf=True)
+        return time.perf_counter() - t0, sino, back
+
+    def sample(self):
+        return (f"{CPU_VIEWS_PER_STEP} views per step of the workload, cycling through 8 fixed view sets: the "
+                f"reference's siddon_3d ProjectFlatKernel + BackProjectFlatKernel device code compiled as host C++ "
+                f"(-O3 -march=x86-64-v3, OpenMP over (view, detector row), atomic adds for the backprojection)")
 
 
 def run_reference(args):
     """--impl reference: the reference's CPU path on the host cores."""
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    views = 2
-    v, kind, cores, sample = cpu_sample(views, args.steps, args.warmup)
+    c = SCANS[args.workload]
+    c["nv"] = args.views or c["nv"]
+    ref = HostReference(c, phantom_xfast(c).numpy())
+    times, inter = [], []
+    for s in range(args.warmup + args.steps):
+        idx = sample_views(c, s)
+        cnt = ref.count(idx)
+        dt, _, _ = ref.step(idx)
+        if s >= args.warmup:
+            times.append(dt)
+            inter.append(2 * cnt)
+    v = sum(inter) / sum(times)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": config_dict({"ranks_running": 1 if ws > 1 else 1}),
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded ellipsoid phantom)", "config": config_dict(c),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": ref.threads(), "kind": ref.kind,
+                             "sample": ref.sample()},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+# ---------------- ceilings of the walks ----------------
+
+def measure_ceilings(dev):
+    """L2 read bandwidth and L2 reduction rate of this GPU (nefct_probe_*),
+    over 32 MiB buffers (L2-resident), best of 3 after a warm-up."""
+    import ctypes as C
+    import torch
+    from nefct_b200 import _lib
+    lib = _lib.load()
+    n = 8 << 20                                   # 32 MiB of floats
+    buf = torch.ones(n, device=dev)
+    sink = torch.empty(int(lib.nefct_probe_sink_floats(8)), device=dev)
+    s = torch.cuda.current_stream(dev).cuda_stream
+    out = {}
+    for name, reps, call in (
+            ("l2_read", 200, lambda r: _lib.call("nefct_probe_l2_read", buf.data_ptr(), n, r, 8, sink.data_ptr(), s)),
+            ("l2_red", 20, lambda r: _lib.call("nefct_probe_l2_red", buf.data_ptr(), n, r, 8, s))):
+        call(2)
+        best = None
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            call(reps)
+            e1.record()
+            e1.synchronize()
+            t = e0.elapsed_time(e1) / 1e3
+            best = t if best is None else min(best, t)
+        out[name] = (reps * n, best)
+    nr, tr = out["l2_read"]
+    nd, td = out["l2_red"]
+    del buf, sink
+    return {"l2_read_gbs": 4 * nr / tr / 1e9, "l2_reductions_per_s": nd / td,
+            "how": "nefct_probe_l2_read (16-byte ld.global.cg) and nefct_probe_l2_red (coalesced "
+                   "red.global.add.f32) over 32 MiB, 8 x 148 CTAs of 256 threads, best of 3"}
 
 
 # ---------------- GPU arm ----------------
@@ -212,35 +297,40 @@ def run_reference(args):
 def run_gpu(args):
     import torch
     import nefct_b200 as nb
-    from nefct_b200 import ops
+    from nefct_b200 import _lib, autotune, ops
 
-    rank, ws, local = dist_setup(args.gpus)
+    c = SCANS[args.workload]
+    c["nv"] = args.views or c["nv"]
+    legs = set(args.legs.split(","))
+    rank, ws, local = dist_setup()
     dev = torch.device("cuda", local)
-    n = CFG["n"]
-    geom = nb.ConeBeam((n, n, n), angles(), CFG["src_iso"], CFG["src_det"], CFG["na"], CFG["pixel"], CFG["nb"],
-                       CFG["pixel"], size=(n * CFG["voxel"],) * 3)
-    vol = nb.ellipsoid_phantom(n, nb.random_ellipsoids(CFG["ellipsoids"], CFG["seed"] + rank), device=dev)
-    vol = vol.permute(2, 1, 0).contiguous()
+    n = c["n"]
+    ang = angles(c)
+    geom = nb.ConeBeam((n, n, n), ang, c["src_iso"], c["src_det"], c["na"], c["pixel"], c["nb"], c["pixel"],
+                       size=(n * c["voxel"],) * 3)
+    cr = dict(c, seed=c["seed"] + rank)
+    vol = phantom_xfast(cr, device=dev)
     inter = ops.cb_count_intersections(geom, 0, device=dev)
-    rays = CFG["nv"] * CFG["na"] * CFG["nb"]
+    rays = c["nv"] * c["na"] * c["nb"]
+    vbytes, sbytes = 4 * n ** 3, 4 * rays
     sino = torch.empty(geom.sino_shape, device=dev)
     back = torch.empty(geom.vol_shape, device=dev)
     gen = torch.Generator(device=dev).manual_seed(35 + rank)
     grad = torch.rand(geom.sino_shape, device=dev, generator=gen) + 0.5     # dense incoming gradient
     flush = torch.empty(256 * 2 ** 20 // 4, device=dev)
 
-    def step():
-        ops.cb_forward(vol, geom, 0, out=sino)
-        ops.cb_backward(grad, geom, 0, out=back)
+    ceil = measure_ceilings(dev)
 
-    from nefct_b200 import autotune
     if args.rows:
         autotune.apply(args.rows, args.order, args.walk)               # fixed launch shape (profiling)
-        tuned = {"rows": args.rows, "order": args.order, "walk": args.walk, "ms": None}
+        tuned = {"rows": args.rows, "order": args.order, "walk": args.walk, "ms": None, "views": None}
     else:
-        tuned = autotune.tune_cone_beam(geom, 0, dev, use_cache=False)  # untimed launch-shape choice
+        # untimed launch-shape choice on every tune_every-th view of the scan
+        sub = geom.subset(np.arange(0, c["nv"], c["tune_every"]))
+        tuned = dict(autotune.tune_cone_beam(sub, 0, dev, use_cache=False), views=sub.nv)
     for _ in range(args.warmup):
-        step()
+        ops.cb_forward(vol, geom, 0, out=sino)
+        ops.cb_backward(grad, geom, 0, out=back)
     torch.cuda.synchronize()
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
@@ -258,93 +348,226 @@ def run_gpu(args):
         barrier(ws)
         wall = time.perf_counter() - wall0
     t_fwd = sum(a.elapsed_time(b) for a, b, _ in ev) / 1e3
-    t_bwd = sum(b.elapsed_time(c) for _, b, c in ev) / 1e3
+    t_bwd = sum(b.elapsed_time(e) for _, b, e in ev) / 1e3
     t_step = max_over_ranks(t_fwd + t_bwd, ws)
     value = ws * args.steps * 2 * inter / t_step
+    del flush
 
-    # e2e through the public op API with pinned host buffers: every step
-    # copies its volume host->device, runs forward + adjoint and copies the
-    # adjoint volume device->host.  The copies run on their own streams with
-    # double buffers, so step i's upload overlaps step i-1's kernels and its
-    # download overlaps step i+1's (how a pipelined caller drives the API);
-    # every copy lies inside the timed region.
-    h_in = torch.empty(geom.vol_shape, pin_memory=True)
-    h_in.copy_(vol.cpu())
-    h_out = [torch.empty(geom.vol_shape, pin_memory=True) for _ in range(2)]
-    d_in = [torch.empty_like(vol) for _ in range(2)]
-    d_back = [torch.empty_like(vol) for _ in range(2)]
-    ks = torch.cuda.current_stream()
-    hs, ds = torch.cuda.Stream(), torch.cuda.Stream()
+    # e2e through the public op API with pinned host buffers, the traffic of
+    # the drop-in pair (Project3D: volume in, sinogram out; BackProject3D:
+    # sinogram in, volume out): every step uploads its volume and its
+    # incoming gradient sinogram, runs forward + adjoint, and downloads the
+    # forward sinogram and the adjoint volume.  Copies run on their own
+    # streams with double-buffered device tensors, so step i's uploads
+    # overlap step i-1's kernels and its downloads overlap step i+1's; every
+    # copy lies inside the timed region.
+    e2e = None
+    if "e2e" in legs:
+        h_vol = torch.empty(geom.vol_shape, pin_memory=True)
+        h_vol.copy_(vol.cpu())
+        h_grad = torch.empty(geom.sino_shape, pin_memory=True)
+        h_grad.copy_(grad.cpu())
+        h_sino = [torch.empty(geom.sino_shape, pin_memory=True) for _ in range(2)]
+        h_back = [torch.empty(geom.vol_shape, pin_memory=True) for _ in range(2)]
+        d_vol = [torch.empty_like(vol) for _ in range(2)]
+        d_grad = [torch.empty_like(grad) for _ in range(2)]
+        d_sino = [torch.empty_like(sino) for _ in range(2)]
+        d_back = [torch.empty_like(back) for _ in range(2)]
+        ks = torch.cuda.current_stream()
+        hs, ds = torch.cuda.Stream(), torch.cuda.Stream()
 
-    def e2e_steps(n, start):
-        ev_up = [torch.cuda.Event() for _ in range(2)]
-        ev_k = [torch.cuda.Event() for _ in range(2)]
-        ev_down = [torch.cuda.Event() for _ in range(2)]
-        hs.wait_event(start)
-        for i in range(n):
-            b = i % 2
-            if i >= 2:
-                hs.wait_event(ev_k[b])            # step i-2's kernels are done with d_in[b]
-            with torch.cuda.stream(hs):
-                d_in[b].copy_(h_in, non_blocking=True)
-            ev_up[b].record(hs)
-            ks.wait_event(ev_up[b])
-            if i >= 2:
-                ks.wait_event(ev_down[b])         # step i-2's download has read d_back[b]
-            ops.cb_forward(d_in[b], geom, 0, out=sino)
-            ops.cb_backward(grad, geom, 0, out=d_back[b])
-            ev_k[b].record(ks)
-            ds.wait_event(ev_k[b])
-            with torch.cuda.stream(ds):
-                h_out[b].copy_(d_back[b], non_blocking=True)
-            ev_down[b].record(ds)
-        for ev in ev_down:
-            ks.wait_event(ev)
+        def e2e_steps(count, start):
+            ev_up = [torch.cuda.Event() for _ in range(2)]
+            ev_f = [torch.cuda.Event() for _ in range(2)]
+            ev_k = [torch.cuda.Event() for _ in range(2)]
+            ev_dn = [torch.cuda.Event() for _ in range(2)]
+            hs.wait_event(start)
+            for i in range(count):
+                b = i % 2
+                if i >= 2:
+                    hs.wait_event(ev_k[b])        # step i-2's kernels are done with d_vol[b], d_grad[b]
+                with torch.cuda.stream(hs):
+                    d_vol[b].copy_(h_vol, non_blocking=True)
+                    d_grad[b].copy_(h_grad, non_blocking=True)
+                ev_up[b].record(hs)
+                ks.wait_event(ev_up[b])
+                if i >= 2:
+                    ks.wait_event(ev_dn[b])       # step i-2's downloads have read d_sino[b], d_back[b]
+                ops.cb_forward(d_vol[b], geom, 0, out=d_sino[b])
+                ev_f[b].record(ks)
+                ops.cb_backward(d_grad[b], geom, 0, out=d_back[b])
+                ev_k[b].record(ks)
+                ds.wait_event(ev_f[b])
+                with torch.cuda.stream(ds):
+                    h_sino[b].copy_(d_sino[b], non_blocking=True)
+                ds.wait_event(ev_k[b])
+                with torch.cuda.stream(ds):
+                    h_back[b].copy_(d_back[b], non_blocking=True)
+                ev_dn[b].record(ds)
+            for e in ev_dn:
+                ks.wait_event(e)
 
-    w0 = torch.cuda.Event()
-    w0.record(ks)
-    e2e_steps(max(2, args.warmup), w0)
-    torch.cuda.synchronize()
-    barrier(ws)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(ks)
-    e2e_steps(args.steps, e0)
-    e1.record(ks)
-    barrier(ws)
-    t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3, ws)
-    e2e = ws * args.steps * 2 * inter / t_e2e
-    vbytes = int(vol.numel() * 4)
+        w0 = torch.cuda.Event()
+        w0.record(ks)
+        e2e_steps(max(2, args.warmup), w0)
+        torch.cuda.synchronize()
+        barrier(ws)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ks)
+        e2e_steps(args.steps, e0)
+        e1.record(ks)
+        barrier(ws)
+        t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3, ws)
+        e2e = {"value": ws * args.steps * 2 * inter / t_e2e, "unit": UNIT, "h2d_bytes_per_step": vbytes + sbytes,
+               "d2h_bytes_per_step": sbytes + vbytes, "ms_per_step": 1e3 * t_e2e / args.steps}
+        del h_vol, h_grad, h_sino, h_back, d_vol, d_grad, d_sino, d_back
+        torch.cuda.empty_cache()
 
-    # roofline of the dominant op (forward or adjoint) on its algorithmic bytes
+    # rooflines of both kernels against the ceilings measured above: the
+    # HBM copy bandwidth (compulsory bytes), the L2 read bandwidth (forward
+    # gathers) and the L2 reduction rate (transpose)
     peak, peak_kind = load_peaks()
     fwd_s, bwd_s = t_fwd / args.steps, t_bwd / args.steps
     walk = tuned["walk"]
-    if bwd_s >= fwd_s:
-        dom = "cb_colwarp_kernel<transpose>" if walk & 2 else "cb_backward_kernel"
-        dom_t, alg = bwd_s, 8 * inter + 4 * rays
-    else:
-        dom = "cb_colwarp_kernel<forward>" if walk & 1 else "cb_forward_kernel"
-        dom_t, alg = fwd_s, 4 * inter + 4 * rays
-    achieved = alg / dom_t / 1e9
-    traffic = load_traffic().get(dom)
+    names = {"fwd": "cb_colwarp_kernel<forward>" if walk & 1 else "cb_forward_kernel",
+             "bwd": "cb_colwarp_kernel<transpose>" if walk & 2 else "cb_backward_kernel"}
+    traffic = load_traffic(args.workload)
+    roof = {}
+    for d, t, alg, comp in (("fwd", fwd_s, 4 * inter + 4 * rays, vbytes + sbytes),
+                            ("bwd", bwd_s, 8 * inter + 4 * rays, 2 * vbytes + sbytes)):
+        t_hbm = comp / (peak * 1e9)
+        t_l2 = (4 * inter / (ceil["l2_read_gbs"] * 1e9)) if d == "fwd" else inter / ceil["l2_reductions_per_s"]
+        tr = traffic.get(names[d])
+        roof[d] = {"kernel": names[d], "ms": 1e3 * t, "algorithmic_bytes": alg, "compulsory_bytes": comp,
+                   "traffic": tr, "traffic_gbs": tr / t / 1e9 if tr else None,
+                   "t_hbm_ms": 1e3 * t_hbm, "t_l2_ms": 1e3 * t_l2,
+                   "binding": "l2_read" if d == "fwd" and t_l2 >= t_hbm else
+                              "l2_reductions" if t_l2 >= t_hbm else "hbm",
+                   "frac_binding": max(t_hbm, t_l2) / t}
+    dom = "bwd" if bwd_s >= fwd_s else "fwd"
+    rd = roof[dom]
+    achieved = rd["algorithmic_bytes"] / (rd["ms"] / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": rd["kernel"], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "algorithmic_bytes": rd["algorithmic_bytes"],
+                "traffic": rd["traffic"],
+                "traffic_frac_of_hbm": rd["traffic_gbs"] / peak if rd["traffic_gbs"] else None,
+                "binding_ceiling": rd["binding"], "frac_of_binding_ceiling": rd["frac_binding"],
+                "ceilings": ceil, "per_kernel": roof}
 
     extras = {"intersections_per_direction": inter, "rays": rays,
               "forward_ms": 1e3 * fwd_s, "adjoint_ms": 1e3 * bwd_s,
               "forward_intersections_per_s": inter / fwd_s, "adjoint_intersections_per_s": inter / bwd_s,
-              "wall_s_timed_loop": wall, "launch_shape": {"rows_per_cta": tuned["rows"],
-                                                          "grid_order": "row-band outermost" if tuned["order"] == 0
-                                                          else "view outermost",
-                                                          "walk": {"forward": "column warps" if tuned["walk"] & 1
-                                                                   else "thread per ray",
-                                                                   "adjoint": "column warps" if tuned["walk"] & 2
-                                                                   else "thread per ray"},
-                                                          "autotune_ms": tuned["ms"]}}
+              "wall_s_timed_loop": wall,
+              "launch_shape": {"rows_per_cta": tuned["rows"],
+                               "grid_order": "row-band outermost" if tuned["order"] == 0 else "view outermost",
+                               "walk": {"forward": "column warps" if walk & 1 else "thread per ray",
+                                        "adjoint": "column warps" if walk & 2 else "thread per ray"},
+                               "tuned_on_views": tuned.get("views"), "autotune_ms": tuned["ms"]}}
 
-    # FDK of this scanner (256^3, 360 views): line-integral projections of the
-    # phantom, cosine weight + ramp filter + weighted voxel-driven backprojection
-    from nefct_b200 import recon
+    # parity and CPU baseline: the reference's host build on sampled views
+    # of this scan, element-wise against the GPU kernels on the same views
+    cpu = None
+    if rank == 0 and ws == 1 and "parity" in legs:
+        cpu, extras["parity"] = parity_and_baseline(c, geom, vol, dev)
+
+    if "extras" in legs and rank == 0:
+        extras.update(other_scans(c, dev, with_cpu="parity" in legs))
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * t_step / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ellipsoid phantom)",
+                "config": config_dict(c), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": 4 * args.steps, "clocks": clk.summary(), "extras": extras}
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def parity_and_baseline(c, geom, vol, dev):
+    """Times the reference's host build on CPU_VIEWS_PER_STEP-view samples
+    (3 steps) and compares its forward sinograms and backprojections with the
+    GPU's for the same views (rel-L2, max-abs / max); states the GPU
+    forward's error against the oracle's FP64 walk on the first sample."""
+    import torch
+    from nefct_b200 import _lib, ops
+    import oracle
+    ref = HostReference(c, vol.cpu().numpy())
+    tot_i, tot_t = 0, 0.0
+    worst = {"forward_rel_l2": 0.0, "forward_max_abs_over_max": 0.0, "backprojection_rel_l2": 0.0,
+             "backprojection_max_abs_over_max": 0.0}
+
+    def err(a, b):
+        a = np.asarray(a, np.float64)
+        b = np.asarray(b, np.float64)
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b)), float(np.abs(a - b).max() / np.abs(b).max())
+
+    views = []
+    for s in range(3):
+        idx = sample_views(c, s)
+        views += idx
+        cnt = ref.count(idx)
+        dt, r_sino, r_back = ref.step(idx)
+        tot_i += 2 * cnt
+        tot_t += dt
+        sub = geom.subset(idx)
+        g_sino = ops.cb_forward(vol, sub, 0).cpu().numpy()
+        g_back = ops.cb_backward(torch.from_numpy(r_sino).to(dev), sub, _lib.REF_BACKPROJECT).cpu().numpy()
+        for key, (a, b) in (("forward", (g_sino, r_sino)), ("backprojection", (g_back, r_back))):
+            rl, ma = err(a, b)
+            worst[f"{key}_rel_l2"] = max(worst[f"{key}_rel_l2"], rl)
+            worst[f"{key}_max_abs_over_max"] = max(worst[f"{key}_max_abs_over_max"], ma)
+        if s == 0:
+            f64, _ = oracle.cb_forward(ref.g, ref.vol, ref.ang[idx], *ref.args, f64=True)
+            worst["forward_rel_l2_vs_fp64_oracle"], _ = err(g_sino, f64)
+            worst["reference_forward_rel_l2_vs_fp64_oracle"], _ = err(r_sino, f64)
+    worst.update({"views": views, "against": ref.kind, "bar": "rel-L2 <= 1e-5, max-abs <= 1e-4 x max",
+                  "backprojection": "reference backprojection (no 1/L^2) of the reference's own sinogram"})
+    cpu = {"value": tot_i / tot_t, "unit": UNIT, "cores": ref.threads(), "kind": ref.kind,
+           "sample": ref.sample().replace("per step", "per step (3 steps)")}
+    return cpu, worst
+
+
+def other_scans(c, dev, with_cpu=False):
+    """Extras beside the headline: the fwd+adjoint pair on the other scan,
+    and FDK (Ram-Lak, Shepp-Logan, Parker short scan) of the FDK scanner."""
+    import torch
+    import nefct_b200 as nb
+    from nefct_b200 import ops, recon
+    out = {}
+    f = SCANS["fdk-scanner"]
+    n = f["n"]
+    geom = nb.ConeBeam((n, n, n), angles(f), f["src_iso"], f["src_det"], f["na"], f["pixel"], f["nb"], f["pixel"],
+                       size=(n * f["voxel"],) * 3)
+    vol = phantom_xfast(f, device=dev)
+    if c is not f:
+        inter = ops.cb_count_intersections(geom, 0, device=dev)
+        y = torch.rand(geom.sino_shape, device=dev, generator=torch.Generator(device=dev).manual_seed(36)) + 0.5
+        sino, back = torch.empty(geom.sino_shape, device=dev), torch.empty(geom.vol_shape, device=dev)
+        for _ in range(2):
+            ops.cb_forward(vol, geom, 0, out=sino)
+            ops.cb_backward(y, geom, 0, out=back)
+        ef = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        reps = 5
+        ts = [0.0, 0.0]
+        for _ in range(reps):
+            ef[0].record()
+            ops.cb_forward(vol, geom, 0, out=sino)
+            ef[1].record()
+            ops.cb_backward(y, geom, 0, out=back)
+            ef[2].record()
+            torch.cuda.synchronize()
+            ts[0] += ef[0].elapsed_time(ef[1]) / 1e3 / reps
+            ts[1] += ef[1].elapsed_time(ef[2]) / 1e3 / reps
+        out["fdk_scanner_fwd_adjoint"] = {"workload": workload_name(f), "forward_ms": 1e3 * ts[0],
+                                          "adjoint_ms": 1e3 * ts[1],
+                                          "intersections_per_s": 2 * inter / (ts[0] + ts[1])}
+        del y, sino, back
     fdk = {}
     lines = ops.cb_forward(vol, geom, nb._lib.LINE_INTEGRAL)
+    c3 = slice(n // 4, 3 * n // 4)
+    filt_rl = None
     for win in ("ram-lak", "shepp-logan"):
         recon.fdk(lines, geom, win)
         ef = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
@@ -355,65 +578,46 @@ def run_gpu(args):
         ef[2].record()
         torch.cuda.synchronize()
         t_f, t_b = ef[0].elapsed_time(ef[1]) / 1e3, ef[1].elapsed_time(ef[2]) / 1e3
-        c = slice(n // 4, 3 * n // 4)
-        err = float((rec[c, c, c] - vol[c, c, c]).norm() / vol[c, c, c].norm())
+        e = float((rec[c3, c3, c3] - vol[c3, c3, c3]).norm() / vol[c3, c3, c3].norm())
+        if filt_rl is None:
+            filt_rl = filt
         fdk[win] = {"filter_ms": 1e3 * t_f, "backproject_ms": 1e3 * t_b,
-                    "voxels_per_s": n ** 3 / (t_f + t_b), "voxel_views_per_s": n ** 3 * CFG["nv"] / t_b,
-                    "central_rel_error_vs_phantom": err}
-    # the reference's voxel-driven backprojection (pixel_3d: the FDK body
-    # without its distance weight) built for the host, on a 2-view sample
-    # scaled to the scan, beside the GPU backprojection of all views
-    if rank == 0 and ws == 1 and not args.no_cpu:
+                    "voxels_per_s": n ** 3 / (t_f + t_b), "voxel_views_per_s": n ** 3 * f["nv"] / t_b,
+                    "central_rel_error_vs_phantom": e}
+    # short scan 180 deg + fan with Parker weights in the direction the
+    # geometry gives (views spaced like the full scan)
+    fan = 2 * np.degrees(np.arctan(f["na"] * f["pixel"] / 2 / f["src_det"]))
+    step = 360.0 / f["nv"]
+    nss = int(np.ceil((180 + fan) / step)) + 1
+    gss = nb.ConeBeam((n, n, n), np.deg2rad(np.arange(nss) * step - fan / 2), f["src_iso"], f["src_det"],
+                      f["na"], f["pixel"], f["nb"], f["pixel"], size=(n * f["voxel"],) * 3)
+    lss = ops.cb_forward(vol, gss, nb._lib.LINE_INTEGRAL)
+    d = ops.parker_direction(gss)
+    rec = recon.fdk(lss, gss, "ram-lak", d)
+    e = float((rec[c3, c3, c3] - vol[c3, c3, c3]).norm() / vol[c3, c3, c3].norm())
+    fdk["short_scan_parker"] = {"views": nss, "dir": d, "central_rel_error_vs_phantom": e}
+    fdk["workload"] = workload_name(f)
+    if with_cpu:
+        # the reference's voxel-driven backprojection (pixel_3d: the FDK body
+        # without its distance weight) built for the host, on a 2-view
+        # sample scaled to the scan, beside the GPU backprojection
         import oracle
         if oracle.have_ref():
-            hs = filt[:2].cpu().numpy()
-            side = n * CFG["voxel"]
+            hs = filt_rl[:2].cpu().numpy()
+            side = n * f["voxel"]
             t0 = time.perf_counter()
-            oracle.ref_pixel_backproject(hs, angles()[:2], (n, n, n), (-side / 2,) * 3, (side,) * 3,
-                                         CFG["src_iso"], CFG["src_det"], CFG["na"], CFG["pixel"], 0.0,
-                                         CFG["nb"], CFG["pixel"], 0.0)
-            t_host = (time.perf_counter() - t0) * CFG["nv"] / 2
-            fdk["reference_host_build"] = {"cores": os.cpu_count(), "sample": "2 views, scaled to the scan",
+            oracle.ref_pixel_backproject(hs, angles(f)[:2], (n, n, n), (-side / 2,) * 3, (side,) * 3,
+                                         f["src_iso"], f["src_det"], f["na"], f["pixel"], 0.0, f["nb"], f["pixel"],
+                                         0.0)
+            t_host = (time.perf_counter() - t0) * f["nv"] / 2
+            t_b = fdk["ram-lak"]["backproject_ms"] / 1e3
+            fdk["reference_host_build"] = {"cores": oracle.ref_threads(), "sample": "2 views, scaled to the scan",
                                            "pixel_backproject_ms": 1e3 * t_host,
                                            "speedup_of_fdk_backproject": t_host / t_b}
-    # short scan 180 deg + fan with Parker weights (views spaced like the full scan)
-    fan = 2 * np.degrees(np.arctan(CFG["na"] * CFG["pixel"] / 2 / CFG["src_det"]))
-    step = 360.0 / CFG["nv"]
-    nss = int(np.ceil((180 + fan) / step)) + 1
-    gss = nb.ConeBeam((n, n, n), np.deg2rad(np.arange(nss) * step - fan / 2), CFG["src_iso"], CFG["src_det"],
-                      CFG["na"], CFG["pixel"], CFG["nb"], CFG["pixel"], size=(n * CFG["voxel"],) * 3)
-    lss = ops.cb_forward(vol, gss, nb._lib.LINE_INTEGRAL)
-    best = None
-    for d in (1, -1):
-        rec = recon.fdk(lss, gss, "ram-lak", d)
-        c = slice(n // 4, 3 * n // 4)
-        err = float((rec[c, c, c] - vol[c, c, c]).norm() / vol[c, c, c].norm())
-        best = (err, d) if best is None or err < best[0] else best
-    fdk["short_scan_parker"] = {"views": nss, "dir": best[1], "central_rel_error_vs_phantom": best[0]}
-    del lines, filt, rec, lss
-    extras["fdk"] = fdk
-
-    cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu:
-        v, kind, cores, sample = cpu_sample(2, 3)
-        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
-
-    if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": 1e3 * t_step / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ellipsoid phantom)",
-                "config": config_dict(),
-                "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "peak_source": peak_kind,
-                             "algorithmic_bytes": alg, "traffic": traffic},
-                "cpu_baseline": cpu,
-                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": vbytes, "d2h_bytes_per_step": vbytes},
-                "gpu_launches": 4 * args.steps,
-                "clocks": clk.summary(), "extras": extras}
-        print(json.dumps(line), flush=True)
-    if ws > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    out["fdk"] = fdk
+    del lines, filt, filt_rl, rec, lss, vol
+    torch.cuda.empty_cache()
+    return out
 
 
 # ---------------- batched uneven problems (64 problems, edges 64..384) ----------------
@@ -628,6 +832,7 @@ def run_rows(args):
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
     gen = torch.Generator(device=dev).manual_seed(9)
+    CFG = SCANS["fdk-scanner"]
     n = CFG["n"]
 
     def timed(fn, reps=None):
@@ -664,7 +869,7 @@ def run_rows(args):
                         "walk_order": "ordered (lor_order, computed once per list)", "order_ms": 1e3 * t_ord,
                         "list_order_forward_ms": 1e3 * t_lf0, "list_order_backward_ms": 1e3 * t_lb0}
     # reference backprojection / deterministic / exact on 36 views of the bench scanner
-    ang = angles()[::10]
+    ang = angles(CFG)[::10]
     g = nb.ConeBeam((n, n, n), ang, CFG["src_iso"], CFG["src_det"], CFG["na"], CFG["pixel"], CFG["nb"],
                     CFG["pixel"], size=(n * CFG["voxel"],) * 3)
     y = torch.rand(g.sino_shape, device=dev, generator=gen)
@@ -696,7 +901,7 @@ def run_rows(args):
                             "adjoint_ms": 1e3 * t_wa, "dvf_gradient_ms": 1e3 * t_wg,
                             "invert_30_passes_ms": 1e3 * t_wi}
     # distance-driven FDK backprojection: the bench scanner in voxel units, 72 views
-    ang72 = angles()[::5]
+    ang72 = angles(CFG)[::5]
     proj = torch.rand((ang72.size, CFG["nb"], CFG["na"]), device=dev, generator=gen)
     px = CFG["pixel"] / CFG["voxel"]
     sad, sid = CFG["src_iso"] / CFG["voxel"], CFG["src_det"] / CFG["voxel"]
@@ -721,7 +926,7 @@ def run_rows(args):
             oracle.ref_dd_backproject(ph, ang72[:2], (n, n, n), sid, sad, CFG["na"], px, 0.0, CFG["nb"], px, 0.0)
             t_cpu_dd = (time.perf_counter() - t0) * ang72.size / 2
             rows["reference_host_build"] = {
-                "cores": os.cpu_count(), "lor_forward_lors_per_s": k / t_cpu_lor,
+                "cores": oracle.ref_threads(), "lor_forward_lors_per_s": k / t_cpu_lor,
                 "lor_forward_speedup": (nl / t_lf) / (k / t_cpu_lor),
                 "warp_forward_ms": 1e3 * t_cpu_warp, "warp_forward_speedup": t_cpu_warp / t_wf,
                 "distance_driven_72_views_ms_from_2_view_sample": 1e3 * t_cpu_dd,
@@ -740,21 +945,30 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
-    ap.add_argument("--views", type=int, default=360, help="views of the scan (360 = the workload; fewer only for profiling)")
+    ap.add_argument("--workload", default="diff-projector",
+                    choices=["diff-projector", "fdk-scanner", "batched", "diff512", "motion4d", "rows"],
+                    help="diff-projector: the headline scan (512^3, 720 views); fdk-scanner: the same step on the "
+                         "256^3 / 360-view scanner; the others print their own JSON lines")
+    ap.add_argument("--legs", default="e2e,parity,extras",
+                    help="parts of the scan workloads besides the timed loop: e2e (host copies), parity (reference "
+                         "host build on sampled views, CPU baseline), extras (the other scan, FDK)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the reference host-build legs")
+    ap.add_argument("--views", type=int, default=0, help="views of the scan (0 = the workload's; fewer only for "
+                                                         "profiling)")
     ap.add_argument("--rows", type=int, default=0, help="fix the detector rows per CTA instead of autotuning")
-    ap.add_argument("--order", type=int, default=1, help="with --rows: 0 row bands outermost, 1 views outermost")
+    ap.add_argument("--order", type=int, default=0, help="with --rows: 0 row bands outermost, 1 views outermost")
     ap.add_argument("--walk", type=int, default=3,
                     help="with --rows: column warps for the forward (bit 0) / adjoint (bit 1), else thread per ray")
-    ap.add_argument("--workload", default="fdk-scanner",
-                    choices=["fdk-scanner", "batched", "diff512", "motion4d", "rows"],
-                    help="batched: the 64 uneven problems (its own JSON line)")
     ap.add_argument("--problems", type=int, default=64)
     ap.add_argument("--scale", type=float, default=1.0, help="batched: scale of volume edges and detector sizes")
     ap.add_argument("--view-scale", type=float, default=1.0, help="batched: scale of the view counts")
     args = ap.parse_args()
-    CFG["nv"] = args.views
+    if args.no_cpu:
+        args.legs = ",".join(x for x in args.legs.split(",") if x != "parity")
     if args.impl == "reference":
+        if args.workload not in SCANS:
+            print(json.dumps({"impl": "reference", "unavailable": f"no reference arm for workload {args.workload}"}))
+            return
         run_reference(args)
     elif args.workload == "batched":
         run_batched(args)

@@ -150,17 +150,20 @@ nefct_status nefct_cb_backward(const nefct_cb_geom *g, const float *sino, float 
                                void *workspace, size_t workspace_bytes, void *stream);
 
 /* Forward projection for callers that cannot allocate device memory: the
- * same result as nefct_cb_forward, but its scratch (the y-fastest copy of
- * the volume) lives in a fixed 32 MiB array inside the library instead of a
+ * same kernels and bit-identical result as nefct_cb_forward (same flags,
+ * same launch tuning), but its scratch (the volume copy the walk gathers
+ * from) lives in a fixed 32 MiB array inside the library instead of a
  * caller workspace.  No counterpart in the reference.  It is for callers
  * that may not call cudaMalloc -- a service that reserves all GPU memory at
  * start-up, a host framework that owns the memory pool, a binding that only
  * receives device pointers.  It allocates nothing (no cudaMalloc/cudaFree,
  * no allocating library call) and rejects grids of more than 8 Mi voxels
  * (8388608) with NEFCT_ERR_INVALID.  Every GPU that loads the library holds
- * the 32 MiB until the process exits.  The first call on a device looks up
- * the array's device address (cudaGetSymbolAddress) with that device
- * current; make that first call before any stream capture.  All calls share
+ * the 32 MiB until the process exits.  The first call in each CUDA context
+ * (each device's primary context, a caller's own driver-API context, the new
+ * primary context after cudaDeviceReset) looks up the array's device address
+ * there (cudaGetSymbolAddress) and caches it by the context's ID; make that
+ * first call before any stream capture.  All calls share
  * the one array: calls that overlap on the GPU (other streams, other host
  * threads) race on it and must be serialised by the caller.  Nothing in it
  * needs clearing: each call overwrites every element it reads. */

@@ -622,26 +622,81 @@ static nefct_status lor_impl(const nefct_grid *grid, const T *lors, int64_t n, c
 static constexpr size_t kStaticScratchFloats = size_t(8) << 20;   // 8 Mi voxels
 static __device__ __align__(256) float g_static_scratch[kStaticScratchFloats];
 
-// Host code cannot use g_static_scratch's name as a device address; its
-// address on each device is looked up once, with that device current.
-static constexpr int kMaxDevices = 64;
+// Host code cannot use g_static_scratch's name as a device address.  The
+// address belongs to the CUDA context the library's device code is loaded
+// in, so it is cached per context, keyed by the context's unique ID
+// (cuCtxGetId: never reused within a process), and looked up again
+// (cudaGetSymbolAddress) for a context not seen before: the first call in a
+// process, on another device, under a caller's own driver-API context, or
+// after cudaDeviceReset replaced the device's primary context.  The driver
+// calls are reached through cudaGetDriverEntryPoint (no link to libcuda).
+using CtxGetCurrentFn = int (*)(void **ctx);
+using CtxGetIdFn = int (*)(void *ctx, unsigned long long *id);
+static constexpr int kMaxContexts = 64;
 static std::mutex g_static_mu;
-static float *g_static_addr[kMaxDevices];
+static CtxGetCurrentFn g_ctx_get_current = nullptr;
+static CtxGetIdFn g_ctx_get_id = nullptr;
+static unsigned long long g_static_ctx[kMaxContexts];
+static float *g_static_addr[kMaxContexts];
+static int g_static_n = 0, g_static_next = 0;
+
+// ID of the context current on this thread (have = false: none is current).
+// Call with g_static_mu held.
+static nefct_status current_context_id(bool &have, unsigned long long &id)
+{
+    if (!g_ctx_get_current || !g_ctx_get_id) {
+        void *f1 = nullptr, *f2 = nullptr;
+        cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = q1;
+        cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetDriverEntryPoint(cuCtxGetCurrent)");
+        e = cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetDriverEntryPoint(cuCtxGetId)");
+        if (q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f1 || !f2)
+            return fail(NEFCT_ERR_UNSUPPORTED, "the driver lacks cuCtxGetCurrent / cuCtxGetId (CUDA 12.0+ needed)");
+        g_ctx_get_current = (CtxGetCurrentFn)f1;
+        g_ctx_get_id = (CtxGetIdFn)f2;
+    }
+    void *ctx = nullptr;
+    if (g_ctx_get_current(&ctx) != 0) return fail(NEFCT_ERR_CUDA, "cuCtxGetCurrent failed");
+    have = ctx != nullptr;
+    if (have && g_ctx_get_id(ctx, &id) != 0) return fail(NEFCT_ERR_CUDA, "cuCtxGetId failed");
+    return NEFCT_OK;
+}
 
 static nefct_status static_scratch_address(float **addr)
 {
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-    if (dev < 0 || dev >= kMaxDevices) return fail(NEFCT_ERR_UNSUPPORTED, "device %d out of range", dev);
     std::lock_guard<std::mutex> lock(g_static_mu);
-    if (!g_static_addr[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_static_scratch);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_static_scratch)");
-        g_static_addr[dev] = (float *)p;
+    bool have = false;
+    unsigned long long id = 0;
+    nefct_status st = current_context_id(have, id);
+    if (st) return st;
+    if (have) {
+        for (int i = 0; i < g_static_n; ++i)
+            if (g_static_ctx[i] == id) {
+                *addr = g_static_addr[i];
+                return NEFCT_OK;
+            }
     }
-    *addr = g_static_addr[dev];
+    // a context not seen yet (or none current: the lookup initialises the
+    // device's primary context and makes it current)
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_static_scratch)");
+    if (!have) {
+        st = current_context_id(have, id);
+        if (st) return st;
+        if (!have) return fail(NEFCT_ERR_CUDA, "no CUDA context is current after cudaGetSymbolAddress");
+    }
+    int slot = -1;
+    for (int i = 0; i < g_static_n; ++i)
+        if (g_static_ctx[i] == id) slot = i;
+    if (slot < 0) {
+        slot = g_static_n < kMaxContexts ? g_static_n++ : g_static_next;
+        g_static_next = (g_static_next + 1) % kMaxContexts;
+    }
+    g_static_ctx[slot] = id;
+    g_static_addr[slot] = (float *)p;
+    *addr = (float *)p;
     return NEFCT_OK;
 }
 
@@ -659,12 +714,16 @@ static nefct_status cb_forward_static_impl(const nefct_cb_geom *g, const float *
                     "nefct_cb_forward_noalloc handles at most %zu voxels (its fixed scratch is %zu MiB); this grid "
                     "has %zu -- use nefct_cb_forward with a workspace",
                     kStaticScratchFloats, kStaticScratchFloats * sizeof(float) >> 20, nvox);
+    // the walk nefct_cb_forward takes for these flags and the current
+    // launch tuning, over the same kind of volume copy, so the two give the
+    // same bits
+    const bool cw = cb_use_colwarp<float>(g->grid, flags, true);
     float *scratch = nullptr;
     if (tr) {
         st = static_scratch_address(&scratch);
         if (st) return st;
-        // the transpose overwrites every scratch element this call reads
-        st = transpose_xy(vol, scratch, g->grid, s);
+        // the copy overwrites every scratch element this call reads
+        st = cw ? zmajor_copy(vol, scratch, g->grid, s) : transpose_xy(vol, scratch, g->grid, s);
         if (st) return st;
     }
     CBParams<float> p;            // on the host stack: no allocation of any kind
@@ -675,7 +734,7 @@ static nefct_status cb_forward_static_impl(const nefct_cb_geom *g, const float *
     for (int v0 = 0; v0 < g->nv; v0 += ViewTable<float>::kMax) {
         const int nvc = std::min(ViewTable<float>::kMax, g->nv - v0);
         fill_views(p, g, v0, nvc);
-        const cudaError_t e = cb_launch_forward<float>(p, g->na, g->nb, nvc, flags, s, false);
+        const cudaError_t e = cb_launch_forward<float>(p, g->na, g->nb, nvc, flags, s, cw);
         if (e != cudaSuccess) return cuda_fail(e, "cb_forward_kernel (noalloc)");
     }
     return NEFCT_OK;
@@ -789,8 +848,9 @@ nefct_status nefct_lor_backward_ordered(const nefct_grid *grid, const float *lor
     return lor_impl<float>(grid, lors, n, vals, vol, flags, (cudaStream_t)stream, false, order);
 }
 
-// See cb_forward_static_impl: same result as nefct_cb_forward, with the
-// scratch in the library's fixed device array instead of a caller workspace.
+// See cb_forward_static_impl: the same kernels and result as
+// nefct_cb_forward, with the scratch in the library's fixed device array
+// instead of a caller workspace.
 nefct_status nefct_cb_forward_noalloc(const nefct_cb_geom *g, const float *vol, float *sino, uint32_t flags,
                                       void *stream)
 {

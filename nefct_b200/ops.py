@@ -265,6 +265,25 @@ def fdk_filter(sino: torch.Tensor, geom: ConeBeam, window: str | int = "ram-lak"
     return out
 
 
+def parker_direction(geom: ConeBeam) -> int:
+    """ParkerWeight.m's ``dir`` for this scan: +1 when the view angles
+    increase, -1 when they decrease.
+
+    The ray through detector coordinate a at view angle phi points along
+    phi + g, g = atan(a / src_det) (a grows counter-clockwise: the detector
+    offset is along (-sin phi, cos phi)), so its conjugate ray is measured at
+    view phi + pi + 2 g with fan angle -g.  ParkerWeight.m's
+    pweight = beta - fanang + dir * g (degrees, beta = view index * dang)
+    moves by exactly 180 between a ray and its conjugate -- so that its sin^2
+    and cos^2 ramps add to one over every redundant pair -- only for
+    dir = +1 when beta grows with the angle; a scan that turns the other way
+    walks beta backwards and needs dir = -1."""
+    a = np.asarray(geom.angles, np.float64)
+    if a.size < 2 or a[1] == a[0]:
+        raise NefctError(_lib.ERR_INVALID, "Parker weighting needs at least two distinct view angles")
+    return 1 if a[1] > a[0] else -1
+
+
 def fdk_backproject(filtered: torch.Tensor, geom: ConeBeam, weight: bool = True) -> torch.Tensor:
     """Voxel-driven bilinear backprojection (pixel_3d semantics) with the FDK
     distance weight (backprojection.m) unless weight=False."""

@@ -87,7 +87,9 @@ def sirt(b: torch.Tensor, geom: ops.ConeBeam, n_iter: int, flags: int = _lib.LIN
 def cg(b: torch.Tensor, geom: ops.ConeBeam, n_iter: int, flags: int = _lib.LINE_INTEGRAL, x0=None,
        callback=None, graph: bool = False) -> torch.Tensor:
     """Conjugate gradients on A^T A x = A^T b; alpha and beta stay 0-dim
-    device tensors, so an iteration never waits for the host."""
+    device tensors, so an iteration never waits for the host.  Once the
+    residual is exactly zero (a zero right-hand side, or exact
+    convergence) both step sizes are 0 and the iterate stays put."""
     ax = torch.empty_like(b)
     aty = ops.cb_backward(b, geom, flags)
     x = torch.zeros(geom.vol_shape, device=b.device, dtype=b.dtype) if x0 is None else x0.clone()
@@ -106,13 +108,18 @@ def cg(b: torch.Tensor, geom: ops.ConeBeam, n_iter: int, flags: int = _lib.LINE_
 
     rsold = dot(r, r)
 
+    zero = torch.zeros((), dtype=torch.float64, device=b.device)
+
+    def safe_div(num, den):                       # 0 where den is 0 (converged: r = 0 or p = 0)
+        return torch.where(den > 0, num / torch.where(den > 0, den, torch.ones_like(den)), zero)
+
     def step():
         ap = normal(p)
-        alpha = rsold / dot(p, ap)
+        alpha = safe_div(rsold, dot(p, ap))
         x.add_(p * alpha.float())
         r.sub_(ap * alpha.float())
         rsnew = dot(r, r)
-        p.mul_((rsnew / rsold).float()).add_(r)
+        p.mul_(safe_div(rsnew, rsold).float()).add_(r)
         rsold.copy_(rsnew)
 
     _iterate(step, n_iter, graph, callback, x)

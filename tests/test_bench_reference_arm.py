@@ -22,3 +22,9 @@ def test_reference_arm_prints_contract_line():
     assert line["cpu_baseline"]["kind"] in ("reference", "port") and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
     assert line["e2e"]["value"] == line["value"]
+    assert line["ms_per_step"] > 0
+    # both arms print the same config dict for the same workload
+    sys.path.insert(0, ROOT)
+    import bench
+    assert line["config"] == bench.config_dict(bench.SCANS["diff-projector"])
+    assert line["metric"] == bench.METRIC and line["unit"] == bench.UNIT

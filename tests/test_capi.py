@@ -135,3 +135,15 @@ def test_dd_rejects_bad_geometry(nefct_lib):
     assert nefct_lib.nefct_dd_backproject(C.byref(g), C.c_void_p(16), C.c_void_p(32), C.c_void_p(64), ws, None) == 1
     g.det_kind = 0
     assert nefct_lib.nefct_dd_backproject(C.byref(g), C.c_void_p(16), C.c_void_p(32), C.c_void_p(64), 4, None) == 3
+
+
+def test_noalloc_refuses_grids_beyond_its_scratch(nefct_lib):
+    """The allocation-free forward checks the grid against its fixed 32 MiB
+    scratch before any CUDA call."""
+    import nefct_b200 as nb
+    from nefct_b200 import _lib
+    g = nb.ConeBeam((256, 256, 256), [0.0], 600.0, 1200.0, 64, 1.0, 64, 1.0)
+    s = g.struct()
+    st = nefct_lib.nefct_cb_forward_noalloc(C.byref(s), C.c_void_p(256), C.c_void_p(256), 0, None)
+    assert st == _lib.ERR_INVALID
+    assert b"at most 8388608 voxels" in nefct_lib.nefct_last_error()

@@ -69,3 +69,33 @@ def test_cosine_weight_is_one_on_axis():
     assert L == 64
     out = fdk.fdk_filter(sino, 1e9, 1e9, 1.0, 1.0)
     assert np.isfinite(out).all()
+
+
+@pytest.mark.parametrize("direction,ok", [(1, True), (-1, False)])
+def test_parker_direction_weights_conjugate_pairs_to_one(direction, ok):
+    """The Parker direction of a scan whose angles increase is +1.
+
+    With this geometry's convention the ray at view phi through fan angle g
+    has its conjugate at view phi + 180 + 2 g (degrees) with fan angle -g.
+    Fan angles of whole degrees and a 1-degree view step put every conjugate
+    on a measured view (2 g whole views later), and an even view count keeps
+    every pweight off the region boundaries of ParkerWeight.m (where its
+    three cases leave a weight of 1).  With dir = +1 the weights of every
+    redundant pair add to one; with dir = -1 they do not."""
+    DSD = 1000.0
+    g = np.arange(-5, 6)
+    us = DSD * np.tan(np.deg2rad(g.astype(float)))
+    n_proj = 192
+    W = fdk.parker_weights(us, DSD, 1.0, n_proj, direction)
+    errs = [W[i, j] + W[i + 180 + 2 * gj, len(g) - 1 - j] - 1
+            for i in range(n_proj) for j, gj in enumerate(g) if 0 <= i + 180 + 2 * gj < n_proj]
+    assert len(errs) > 100
+    assert (np.abs(errs).max() < 1e-12) == ok
+
+
+def test_parker_direction_of_geometry():
+    import nefct_b200 as nb
+    from nefct_b200 import ops
+    up = nb.ConeBeam((8, 8, 8), np.linspace(0, 3.6, 10), 100.0, 200.0, 16, 1.0, 8, 1.0)
+    down = nb.ConeBeam((8, 8, 8), np.linspace(0, -3.6, 10), 100.0, 200.0, 16, 1.0, 8, 1.0)
+    assert ops.parker_direction(up) == 1 and ops.parker_direction(down) == -1

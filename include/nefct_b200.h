@@ -338,6 +338,31 @@ size_t nefct_dd_workspace_bytes(const nefct_dd_geom *g);
 nefct_status nefct_dd_backproject(const nefct_dd_geom *g, const float *proj, float *vol, void *ws, size_t ws_bytes,
                                   void *stream);
 
+/* ---- distance-driven projector pair ----
+ * The forward half of the dist_3d_mod family that the reference's
+ * Project3D loads (project_flat_three / project_cyli_three,
+ * nefct/functions/project.py:11-16, :95); its source is not in the
+ * reference, so the forward is defined as the exact transpose of the
+ * backprojection above: each bin (ia, ib, iv) sums voxel * weight over the
+ * voxels and weights its backprojection would spread value into (same
+ * geometry struct, same footprints).  flags: 0 keeps the FDK weight
+ * src_iso^2 / (src_iso + x cos + y sin)^2 in the weight (the transpose of
+ * nefct_dd_backproject); NEFCT_FDK_NO_WEIGHT drops it (footprint-weighted
+ * line integrals, overlap fractions times |p2 - p1| / |driving component|).
+ * nefct_dd_backward with the same flags is the transpose of nefct_dd_forward
+ * (with flags 0 it is nefct_dd_backproject).  proj is [nv][nb][na], vol
+ * [nz][ny][nx]; outputs are overwritten.  Workspace:
+ * nefct_dd_workspace_bytes (a z-fastest volume copy / accumulator).  The
+ * FP64 builds (adjoint and finite-difference checks) need no workspace. */
+nefct_status nefct_dd_forward(const nefct_dd_geom *g, const float *vol, float *proj, uint32_t flags, void *ws,
+                              size_t ws_bytes, void *stream);
+nefct_status nefct_dd_backward(const nefct_dd_geom *g, const float *proj, float *vol, uint32_t flags, void *ws,
+                               size_t ws_bytes, void *stream);
+nefct_status nefct_dd_forward_f64(const nefct_dd_geom *g, const double *vol, double *proj, uint32_t flags,
+                                  void *stream);
+nefct_status nefct_dd_backward_f64(const nefct_dd_geom *g, const double *proj, double *vol, uint32_t flags,
+                                   void *stream);
+
 /* ---- ceiling probes (measurement; no counterpart in the reference) ----
  * The cone-beam walks read and reduce mostly L2-resident data, so their
  * rooflines are set by the L2 read bandwidth and the L2 reduction rate of

@@ -3,7 +3,8 @@
 Cone-beam ray-driven (slab-split "Siddon") forward projector, its exact
 transpose and the reference's own backprojection, the LOR projector pair,
 FDK (cosine/Parker weighting, ramp filtering, voxel-driven weighted
-backprojection) and the cpp/deform trilinear warp -- hand-written CUDA
+backprojection), the distance-driven projector pair and the cpp/deform
+trilinear warp -- hand-written CUDA
 kernels behind the C ABI of include/nefct_b200.h, wrapped as torch ops with
 autograd and as drop-ins for the reference's python operators.
 
@@ -17,7 +18,7 @@ from .geometry import (DetectorConfig, DetectorDirectAConfig, DetectorDirectBCon
 from .data import (Image, Image3D, Image3DT, ProjectionSequence3D, all_one_image, all_zero_image,
                    ellipsoid_phantom, phantom, random_ellipsoids)
 from . import ops
-from .ops import ConeBeam, backproject, project, warp
+from .ops import ConeBeam, DDGeometry, backproject, dd_project, project, warp
 from .functions import (FDK, SART, BackProject3D, BackProject3DT, ConjGrad, Project3D, Project3DT,
                         WarpDeformer, cone_beam)
 from . import cc

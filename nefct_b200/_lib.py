@@ -114,6 +114,10 @@ _PROTOS = {
     "nefct_warp_grad_dvf_f64": (_i32, [_vp, _vp, _vp, _vp, _vp, _i32, _i32, _i32, _vp, _vp, _vp, _vp]),
     "nefct_dd_workspace_bytes": (C.c_size_t, [C.POINTER(DDGeom)]),
     "nefct_dd_backproject": (_i32, [C.POINTER(DDGeom), _vp, _vp, _vp, C.c_size_t, _vp]),
+    "nefct_dd_forward": (_i32, [C.POINTER(DDGeom), _vp, _vp, _u32, _vp, C.c_size_t, _vp]),
+    "nefct_dd_backward": (_i32, [C.POINTER(DDGeom), _vp, _vp, _u32, _vp, C.c_size_t, _vp]),
+    "nefct_dd_forward_f64": (_i32, [C.POINTER(DDGeom), _vp, _vp, _u32, _vp]),
+    "nefct_dd_backward_f64": (_i32, [C.POINTER(DDGeom), _vp, _vp, _u32, _vp]),
     "nefct_probe_sink_floats": (C.c_size_t, [_i32]),
     "nefct_probe_l2_read": (_i32, [_vp, C.c_size_t, _i32, _i32, _vp, _vp]),
     "nefct_probe_l2_red": (_i32, [_vp, C.c_size_t, _i32, _i32, _vp]),

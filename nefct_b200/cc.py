@@ -15,7 +15,16 @@ and output shapes as the registered ops, including their quirks:
 * ``distance_3d`` nefct/cc/distance_3d/dist_3d_back_fdk.cu.cc:257-298 --
   back_project_flat_fdk_gpu / back_project_cyli_fdk_gpu (host entry points
   of the distance-driven FDK backprojection; the reference registers no op
-  for them).  They add into the caller's ``image``, as there.
+  for them).  They add into the caller's ``image``, as there.  Also
+  project_flat_three / project_cyli_three, the forward ops of dist_3d_mod
+  that nefct/functions/project.py:11-16, :88-97 calls with keyword attrs
+  (shape, offsets, angles, SID, SAD, na, da, ai, nb, db, bi; voxel units,
+  SID = source-detector, SAD = source-axis, ai/bi physical offsets in
+  voxels): the reference ships no source for them, so they are this
+  library's distance-driven line integrals (nefct_dd_forward without the
+  FDK weight: footprint overlap fractions times |p2 - p1| / |driving
+  component|, summed per bin), whose exact transpose is
+  nefct_dd_backward.
 
 Tensors are CUDA torch tensors.  ``grid``/``center``/``size`` may be
 sequences or tensors; the reference reads them back from the device with
@@ -161,5 +170,26 @@ def _dd_backproject(cyl):
     return op
 
 
+def _dd_project(cyl):
+    def op(image, shape, offsets, angles, SID, SAD, na, da, ai, nb, db, bi):
+        """image: the volume over x-fastest memory (the transposed numpy /
+        [nz, ny, nx] tensor the reference hands over); returns [nv, nb, na].
+        The bin centre is (i + 0.5) * d + ai - n * d / 2, as in the
+        backprojection of dist_3d_back_fdk.cu.cc:45-60."""
+        nx, ny, nz = (int(v) for v in shape)
+        ang = _angles(angles)
+        off = None if offsets is None else _angles(offsets)
+        if off is not None and off.size == 1 and ang.size > 1:
+            off = np.full(ang.size, off[0], np.float32)
+        g = ops.DDGeometry((nx, ny, nz), ang, float(SAD), float(SID), int(na), float(da), int(nb), float(db),
+                           float(ai), float(bi), "cyl" if cyl else "flat", off)
+        vol = image if isinstance(image, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(image, np.float32))
+        if not vol.is_cuda:
+            vol = vol.cuda()
+        return ops.dd_forward(vol.reshape(nz, ny, nx).contiguous().float(), g, _lib.FDK_NO_WEIGHT)
+    return op
+
+
 distance_3d = types.SimpleNamespace(back_project_flat_fdk_gpu=_dd_backproject(False),
-                                    back_project_cyli_fdk_gpu=_dd_backproject(True))
+                                    back_project_cyli_fdk_gpu=_dd_backproject(True),
+                                    project_flat_three=_dd_project(False), project_cyli_three=_dd_project(True))

@@ -34,139 +34,175 @@
 namespace nefct {
 
 nefct_status zfold(const float *acc, float *vol, const nefct_grid &g, cudaStream_t s);
+nefct_status zmajor_copy(const float *in, float *out, const nefct_grid &g, cudaStream_t s);
 
-struct DDParams {
-    int nx, ny, nz, na, nb, nvc, v0, cyl;
-    float sid, sad;               // source-detector, source-axis (the reference's SID, SAD)
-    float da, ai, db, bi;
-    const float *proj;            // [nv][nb][na], full
-    float *acc;                   // z-fastest [y][x][z]
-    ViewTable<float> tab;
+template <typename T> struct DDParams {
+    int nx, ny, nz, na, nb, nvc, v0, cyl, fdk;
+    T sid, sad;                   // source-detector, source-axis (the reference's SID, SAD)
+    T da, ai, db, bi;
+    const T *src;                 // backward: bins [nv][nb][na] (full); forward: the volume
+    T *dst;                       // backward: accumulator; forward: bins [nv][nb][na] (full)
+    unsigned long long sx, sy, sz;  // volume strides of (ix, iy, iz): z-fastest copy (float) or x-fastest (double)
+    ViewTable<T> tab;
 };
 
 // (i + 0.5) * d + o - n * d / 2 with the reference's promotions: the first
-// part in double, n * d / 2 in float (:45-60)
+// part in double, n * d / 2 in float (:45-60); all double in the FP64 build
 __device__ __forceinline__ float dd_center(int i, float d, float o, int n)
 {
     const float half = __fdiv_rn(__fmul_rn((float)n, d), 2.f);
     return (float)__dsub_rn(__dadd_rn(__dmul_rn((double)i + 0.5, (double)d), (double)o), (double)half);
 }
-
-// i * d + o - n * d / 2 in float (:78-80)
-__device__ __forceinline__ float dd_edge(int i, float d, float o, int n)
+__device__ __forceinline__ double dd_center(int i, double d, double o, int n)
 {
-    return __fsub_rn(__fadd_rn(__fmul_rn((float)i, d), o), __fdiv_rn(__fmul_rn((float)n, d), 2.f));
+    return __dsub_rn(__dadd_rn(__dmul_rn((double)i + 0.5, d), o), __dmul_rn((double)n, d) * 0.5);
 }
 
-// cos/sin of a detector angle: the double-precision functions, rounded
-__device__ __forceinline__ void dd_trig(float a, float &c, float &s)
+// i * d + o - n * d / 2 (:78-80)
+template <typename T> __device__ __forceinline__ T dd_edge(int i, T d, T o, int n)
+{
+    return FP<T>::sub(FP<T>::add(FP<T>::mul((T)i, d), o), FP<T>::div(FP<T>::mul((T)n, d), (T)2));
+}
+
+// cos/sin of a detector angle: the double-precision functions (rounded for float)
+template <typename T> __device__ __forceinline__ void dd_trig(T a, T &c, T &s)
 {
     double sd, cd;
     sincos((double)a, &sd, &cd);
-    c = (float)cd;
-    s = (float)sd;
+    c = (T)cd;
+    s = (T)sd;
 }
 
 // detector point (x20, y20) of lateral coordinate a (flat: a is the offset
 // along the detector; cylindrical: the angle)
-__device__ __forceinline__ void dd_det(const DDParams &p, float a, float &x20, float &y20)
+template <typename T> __device__ __forceinline__ void dd_det(const DDParams<T> &p, T a, T &x20, T &y20)
 {
     if (p.cyl) {
-        float c, s;
+        T c, s;
         dd_trig(a, c, s);
-        x20 = __fsub_rn(__fmul_rn(p.sid, c), p.sad);
-        y20 = __fmul_rn(p.sid, s);
+        x20 = FP<T>::sub(FP<T>::mul(p.sid, c), p.sad);
+        y20 = FP<T>::mul(p.sid, s);
     } else {
-        x20 = __fsub_rn(p.sid, p.sad);
+        x20 = FP<T>::sub(p.sid, p.sad);
         y20 = a;
     }
 }
 
-__device__ __forceinline__ float dd_min(float a, float b) { return a < b ? a : b; }
-__device__ __forceinline__ float dd_max(float a, float b) { return a > b ? a : b; }
-__device__ __forceinline__ float dd_abs(float a) { return a > 0.f ? a : -a; }
+template <typename T> __device__ __forceinline__ T dd_min(T a, T b) { return a < b ? a : b; }
+template <typename T> __device__ __forceinline__ T dd_max(T a, T b) { return a > b ? a : b; }
+template <typename T> __device__ __forceinline__ T dd_abs(T a) { return a > (T)0 ? a : -a; }
+// reciprocal for the weight divisions: approximate in float (<= 1 ulp), exact in double
+__device__ __forceinline__ float dd_rcp(float x) { return rcp_approx(x); }
+__device__ __forceinline__ double dd_rcp(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ int dd_floor(float x) { return (int)floorf(x); }
+__device__ __forceinline__ int dd_floor(double x) { return (int)floor(x); }
 
-__global__ void __launch_bounds__(256) dd_backproject_kernel(const __grid_constant__ DDParams p)
+// One warp walks 32 consecutive rows (bins) of one detector column at one
+// view over the slabs of the column's driving axis.  FWD false: each lane
+// reduces value * weight into the voxels of its bin's footprints (the
+// reference's kernel); FWD true: each lane sums voxel * weight over the same
+// voxels with the same weights (the exact transpose) into its bin.  With
+// p.fdk false the weight lacks the FDK factor SAD^2 / (SAD + x cos + y sin)^2.
+template <typename T, bool FWD>
+__global__ void __launch_bounds__(256) dd_kernel(const __grid_constant__ DDParams<T> p)
 {
+    using F = FP<T>;
     const int lane = threadIdx.x;
     const int ia = blockIdx.x * blockDim.y + threadIdx.y;
     const int ib = blockIdx.y * 32 + lane;
     const int iv = blockIdx.z;
     if (ia >= p.na) return;                       // uniform across the warp
     const bool has = ib < p.nb;
-    const float value = has ? p.proj[((size_t)(p.v0 + iv) * p.nb + ib) * p.na + ia] : 0.f;
-    if (!__any_sync(0xffffffffu, value != 0.f)) return;
-    const bool live = value != 0.f;
+    const size_t bin = ((size_t)(p.v0 + iv) * p.nb + (has ? ib : 0)) * p.na + ia;
+    T value = (T)0;
+    if (!FWD) {
+        value = has ? p.src[bin] : (T)0;
+        if (!__any_sync(0xffffffffu, value != (T)0)) return;
+    }
+    const bool live = FWD ? has : value != (T)0;
 
-    const float cphi = p.tab.cs[iv], sphi = p.tab.sn[iv], off = p.tab.off[iv];
-    const float x1 = __fmul_rn(-p.sad, cphi), y1 = __fmul_rn(-p.sad, sphi), z1 = off;
-    float x20, y20;
+    const T cphi = p.tab.cs[iv], sphi = p.tab.sn[iv], off = p.tab.off[iv];
+    const T x1 = F::mul(-p.sad, cphi), y1 = F::mul(-p.sad, sphi), z1 = off;
+    T x20, y20;
     dd_det(p, dd_center(ia, p.da, p.ai, p.na), x20, y20);
-    const float z20 = dd_center(has ? ib : 0, p.db, p.bi, p.nb);
-    const float x2 = __fsub_rn(__fmul_rn(x20, cphi), __fmul_rn(y20, sphi));
-    const float y2 = __fadd_rn(__fmul_rn(x20, sphi), __fmul_rn(y20, cphi));
-    const float z2 = __fadd_rn(z20, off);
-    const float x21 = __fsub_rn(x2, x1), y21 = __fsub_rn(y2, y1), z21 = __fsub_rn(z2, z1);
+    const T z20 = dd_center(has ? ib : 0, p.db, p.bi, p.nb);
+    const T x2 = F::sub(F::mul(x20, cphi), F::mul(y20, sphi));
+    const T y2 = F::add(F::mul(x20, sphi), F::mul(y20, cphi));
+    const T z2 = F::add(z20, off);
+    const T x21 = F::sub(x2, x1), y21 = F::sub(y2, y1), z21 = F::sub(z2, z1);
     // edges of the bin (the reference recomputes them in every slab)
-    float e[2][2];
+    T e[2][2];
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
-        float ex, ey;
+        T ex, ey;
         dd_det(p, dd_edge(ia + s, p.da, p.ai, p.na), ex, ey);
-        e[s][0] = __fsub_rn(__fsub_rn(__fmul_rn(ex, cphi), __fmul_rn(ey, sphi)), x1);
-        e[s][1] = __fsub_rn(__fadd_rn(__fmul_rn(ex, sphi), __fmul_rn(ey, cphi)), y1);
+        e[s][0] = F::sub(F::sub(F::mul(ex, cphi), F::mul(ey, sphi)), x1);
+        e[s][1] = F::sub(F::add(F::mul(ex, sphi), F::mul(ey, cphi)), y1);
     }
-    const float len = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(x21, x21), __fmul_rn(y21, y21)), __fmul_rn(z21, z21)));
+    const T len = F::sqrt(F::add(F::add(F::mul(x21, x21), F::mul(y21, y21)), F::mul(z21, z21)));
     const bool xdrive = dd_abs(x21) > dd_abs(y21);     // uniform: x21, y21 do not depend on the row
     const int nu = xdrive ? p.nx : p.ny, nvt = xdrive ? p.ny : p.nx;
-    const float u1 = xdrive ? x1 : y1, v1 = xdrive ? y1 : x1, u21 = xdrive ? x21 : y21;
-    const float ul = xdrive ? e[0][0] : e[0][1], vl = xdrive ? e[0][1] : e[0][0];
-    const float ur = xdrive ? e[1][0] : e[1][1], vr = xdrive ? e[1][1] : e[1][0];
+    const T u1 = xdrive ? x1 : y1, v1 = xdrive ? y1 : x1, u21 = xdrive ? x21 : y21;
+    const T ul = xdrive ? e[0][0] : e[0][1], vl = xdrive ? e[0][1] : e[0][0];
+    const T ur = xdrive ? e[1][0] : e[1][1], vr = xdrive ? e[1][1] : e[1][0];
     // the reference divides inside the slab loop; the quotients do not depend on the slab
-    const float r0 = __fdiv_rn(vl, ul), r1 = __fdiv_rn(vl, ur), r2 = __fdiv_rn(vr, ul), r3 = __fdiv_rn(vr, ur);
-    const float hdb = __fdiv_rn(p.db, 2.f);
-    const float rzl = __fdiv_rn(__fsub_rn(z21, hdb), u21), rzr = __fdiv_rn(__fadd_rn(z21, hdb), u21);
-    const float vhalf = (float)(nvt / 2), zhalf = (float)(p.nz / 2), uhalf = __fdiv_rn((float)nu, 2.f);
-    const float len_au = __fdiv_rn(len, dd_abs(u21));
-    const float sad2 = __fmul_rn(p.sad, p.sad);
-    const float xhalf = (float)(p.nx / 2), yhalf = (float)(p.ny / 2);
-    const unsigned zs = (unsigned)p.nz;
+    const T r0 = F::div(vl, ul), r1 = F::div(vl, ur), r2 = F::div(vr, ul), r3 = F::div(vr, ur);
+    const T hdb = F::div(p.db, (T)2);
+    const T rzl = F::div(F::sub(z21, hdb), u21), rzr = F::div(F::add(z21, hdb), u21);
+    const T vhalf = (T)(nvt / 2), zhalf = (T)(p.nz / 2), uhalf = F::div((T)nu, (T)2);
+    const T len_au = F::div(len, dd_abs(u21));
+    const T sad2 = F::mul(p.sad, p.sad);
+    const T xhalf = (T)(p.nx / 2), yhalf = (T)(p.ny / 2);
+    T acc = (T)0;
     for (int iu = 0; iu < nu; ++iu) {
-        const float uc = __fsub_rn(__fsub_rn(__fadd_rn((float)iu, 0.5f), uhalf), u1);
-        const float c0 = __fadd_rn(__fadd_rn(__fmul_rn(r0, uc), v1), vhalf);
-        const float c1 = __fadd_rn(__fadd_rn(__fmul_rn(r1, uc), v1), vhalf);
-        const float c2 = __fadd_rn(__fadd_rn(__fmul_rn(r2, uc), v1), vhalf);
-        const float c3 = __fadd_rn(__fadd_rn(__fmul_rn(r3, uc), v1), vhalf);
-        const float vi1 = dd_min(dd_min(c0, c1), dd_min(c2, c3));
-        const float vi2 = dd_max(dd_max(c0, c1), dd_max(c2, c3));
-        const int va = max(0, (int)floorf(vi1)), vb = min(nvt - 1, (int)floorf(vi2));
+        const T uc = F::sub(F::sub(F::add((T)iu, (T)0.5), uhalf), u1);
+        const T c0 = F::add(F::add(F::mul(r0, uc), v1), vhalf);
+        const T c1 = F::add(F::add(F::mul(r1, uc), v1), vhalf);
+        const T c2 = F::add(F::add(F::mul(r2, uc), v1), vhalf);
+        const T c3 = F::add(F::add(F::mul(r3, uc), v1), vhalf);
+        const T vi1 = dd_min(dd_min(c0, c1), dd_min(c2, c3));
+        const T vi2 = dd_max(dd_max(c0, c1), dd_max(c2, c3));
+        const int va = max(0, dd_floor(vi1)), vb = min(nvt - 1, dd_floor(vi2));
         if (va > vb) continue;                      // uniform: footprint outside the grid
-        const float czl = __fadd_rn(__fadd_rn(__fmul_rn(rzl, uc), z1), zhalf);
-        const float czr = __fadd_rn(__fadd_rn(__fmul_rn(rzr, uc), z1), zhalf);
-        const float zi1 = dd_min(czl, czr), zi2 = dd_max(czl, czr);
-        const int za = max(0, (int)floorf(zi1)), zb = live ? min(p.nz - 1, (int)floorf(zi2)) : -1;
-        const float vspan = __fsub_rn(vi2, vi1), zspan = __fsub_rn(zi2, zi1);
+        const T czl = F::add(F::add(F::mul(rzl, uc), z1), zhalf);
+        const T czr = F::add(F::add(F::mul(rzr, uc), z1), zhalf);
+        const T zi1 = dd_min(czl, czr), zi2 = dd_max(czl, czr);
+        const int za = max(0, dd_floor(zi1)), zb = live ? min(p.nz - 1, dd_floor(zi2)) : -1;
+        const T vspan = F::sub(vi2, vi1), zspan = F::sub(zi2, zi1);
         // the reference's divisions by vspan, zspan and den become
-        // multiplications by approximate reciprocals (<= 1 ulp each)
-        const float ivspan = rcp_approx(vspan), izspan = rcp_approx(zspan);
+        // multiplications by reciprocals (approximate in float: <= 1 ulp each)
+        const T ivspan = dd_rcp(vspan), izspan = dd_rcp(zspan);
         for (int iv2 = va; iv2 <= vb; ++iv2) {
-            const float wv = __fmul_rn(__fsub_rn(dd_min((float)iv2 + 1.0f, vi2), dd_max((float)iv2, vi1)), ivspan);
+            const T wv = F::mul(F::sub(dd_min((T)iv2 + (T)1, vi2), dd_max((T)iv2, vi1)), ivspan);
             const int ix = xdrive ? iu : iv2, iy = xdrive ? iv2 : iu;
-            // (ix + 0.5 - nx / 2): exact in float
-            const float xc = __fsub_rn(__fadd_rn((float)ix, 0.5f), xhalf);
-            const float yc = __fsub_rn(__fadd_rn((float)iy, 0.5f), yhalf);
-            const float den = __fadd_rn(__fadd_rn(p.sad, __fmul_rn(xc, cphi)), __fmul_rn(yc, sphi));
-            const float iden = rcp_approx(den);
-            const float fw = __fmul_rn(__fmul_rn(sad2, iden), iden);
-            // value * wv * (len / |u21|) * fw per voxel of the column, times wz
-            const float cw = __fmul_rn(__fmul_rn(__fmul_rn(value, wv), len_au), fw);
-            float *col = p.acc + ((size_t)iy * p.nx + ix) * zs;
-            for (int iz = za; iz <= zb; ++iz) {
-                const float wz = __fmul_rn(__fsub_rn(dd_min((float)iz + 1.0f, zi2), dd_max((float)iz, zi1)), izspan);
-                atomicAdd(col + iz, __fmul_rn(cw, wz));
+            T fw = (T)1;
+            if (p.fdk) {
+                // (ix + 0.5 - nx / 2): exact
+                const T xc = F::sub(F::add((T)ix, (T)0.5), xhalf);
+                const T yc = F::sub(F::add((T)iy, (T)0.5), yhalf);
+                const T den = F::add(F::add(p.sad, F::mul(xc, cphi)), F::mul(yc, sphi));
+                const T iden = dd_rcp(den);
+                fw = F::mul(F::mul(sad2, iden), iden);
+            }
+            const size_t col = (size_t)iy * p.sy + (size_t)ix * p.sx;
+            if (FWD) {
+                // wv * (len / |u21|) * fw per voxel of the column, times wz
+                const T cw = F::mul(F::mul(wv, len_au), fw);
+                for (int iz = za; iz <= zb; ++iz) {
+                    const T wz = F::mul(F::sub(dd_min((T)iz + (T)1, zi2), dd_max((T)iz, zi1)), izspan);
+                    acc = F::add(acc, F::mul(__ldg(p.src + col + (size_t)iz * p.sz), F::mul(cw, wz)));
+                }
+            } else {
+                // value * wv * (len / |u21|) * fw per voxel of the column, times wz
+                const T cw = F::mul(F::mul(F::mul(value, wv), len_au), fw);
+                for (int iz = za; iz <= zb; ++iz) {
+                    const T wz = F::mul(F::sub(dd_min((T)iz + (T)1, zi2), dd_max((T)iz, zi1)), izspan);
+                    atomicAdd(p.dst + col + (size_t)iz * p.sz, F::mul(cw, wz));
+                }
             }
         }
     }
+    if (FWD && has) p.dst[bin] = acc;
 }
 
 static nefct_status check_dd(const nefct_dd_geom *g)
@@ -189,6 +225,80 @@ static nefct_status check_dd(const nefct_dd_geom *g)
     return NEFCT_OK;
 }
 
+template <typename T>
+static nefct_status dd_impl(const nefct_dd_geom *g, const T *src, T *dst, uint32_t flags, void *ws, size_t ws_bytes,
+                            cudaStream_t s, bool forward)
+{
+    nefct_status st = check_dd(g);
+    if (st) return st;
+    if (!src || !dst) return fail(NEFCT_ERR_INVALID, "input and output must be non-NULL");
+    if (flags & ~NEFCT_FDK_NO_WEIGHT) return fail(NEFCT_ERR_INVALID, "unknown flag bits 0x%x", flags);
+    const bool f32 = sizeof(T) == sizeof(float);
+    const size_t nvox = (size_t)g->nx * g->ny * g->nz;
+    const nefct_grid gr{g->nx, g->ny, g->nz, 0.f, 0.f, 0.f, (float)g->nx, (float)g->ny, (float)g->nz};
+    DDParams<T> *p = new DDParams<T>();
+    p->nx = g->nx; p->ny = g->ny; p->nz = g->nz; p->na = g->na; p->nb = g->nb;
+    p->cyl = g->det_kind == NEFCT_DET_CYL;
+    p->fdk = !(flags & NEFCT_FDK_NO_WEIGHT);
+    p->sid = g->src_det; p->sad = g->src_iso;
+    p->da = g->da; p->ai = g->a_offset; p->db = g->db; p->bi = g->b_offset;
+    if (f32) {
+        // float: a z-fastest volume copy [y][x][z] (forward source / backward
+        // accumulator), so the 32 rows of a warp touch neighbouring z
+        const size_t need = nefct_dd_workspace_bytes(g);
+        if (!ws || ws_bytes < need) {
+            delete p;
+            return fail(NEFCT_ERR_WORKSPACE, "needs %zu workspace bytes, got %zu", need, ws_bytes);
+        }
+        p->sx = (unsigned long long)g->nz;
+        p->sy = (unsigned long long)g->nx * g->nz;
+        p->sz = 1;
+        if (forward) {
+            st = zmajor_copy((const float *)src, (float *)ws, gr, s);
+            if (st) { delete p; return st; }
+            p->src = (const T *)ws;
+            p->dst = dst;
+        } else {
+            const cudaError_t e = cudaMemsetAsync(ws, 0, need, s);
+            if (e != cudaSuccess) { delete p; return cuda_fail(e, "cudaMemsetAsync"); }
+            p->src = src;
+            p->dst = (T *)ws;
+        }
+    } else {
+        // double (checks and tests): the x-fastest volume in place, no workspace
+        p->sx = 1;
+        p->sy = (unsigned long long)g->nx;
+        p->sz = (unsigned long long)g->nx * g->ny;
+        p->src = src;
+        p->dst = dst;
+        if (!forward) {
+            const cudaError_t e = cudaMemsetAsync(dst, 0, nvox * sizeof(T), s);
+            if (e != cudaSuccess) { delete p; return cuda_fail(e, "cudaMemsetAsync"); }
+        }
+    }
+    const int cols = 4;
+    const int kMax = ViewTable<T>::kMax;
+    for (int v0 = 0; v0 < g->nv; v0 += kMax) {
+        const int nvc = std::min(kMax, g->nv - v0);
+        p->v0 = v0;
+        p->nvc = nvc;
+        for (int i = 0; i < nvc; ++i) {
+            const double a = (double)g->angles[v0 + i];
+            p->tab.cs[i] = (T)cos(a);
+            p->tab.sn[i] = (T)sin(a);
+            p->tab.off[i] = g->z_offsets ? (T)g->z_offsets[v0 + i] : (T)0;
+        }
+        dim3 grid((g->na + cols - 1) / cols, (g->nb + 31) / 32, nvc);
+        if (forward) dd_kernel<T, true><<<grid, dim3(32, cols), 0, s>>>(*p);
+        else dd_kernel<T, false><<<grid, dim3(32, cols), 0, s>>>(*p);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) { delete p; return cuda_fail(e, forward ? "dd_kernel<forward>" : "dd_kernel<backward>"); }
+    }
+    delete p;
+    if (f32 && !forward) return zfold((const float *)ws, (float *)dst, gr, s);
+    return NEFCT_OK;
+}
+
 }  // namespace nefct
 
 using namespace nefct;
@@ -204,40 +314,31 @@ size_t nefct_dd_workspace_bytes(const nefct_dd_geom *g)
 nefct_status nefct_dd_backproject(const nefct_dd_geom *g, const float *proj, float *vol, void *ws, size_t ws_bytes,
                                   void *stream)
 {
-    nefct_status st = check_dd(g);
-    if (st) return st;
-    if (!proj || !vol) return fail(NEFCT_ERR_INVALID, "proj and vol must be non-NULL");
-    const size_t need = nefct_dd_workspace_bytes(g);
-    if (!ws || ws_bytes < need) return fail(NEFCT_ERR_WORKSPACE, "needs %zu workspace bytes, got %zu", need, ws_bytes);
-    cudaStream_t s = (cudaStream_t)stream;
-    NEFCT_CHECK_CUDA(cudaMemsetAsync(ws, 0, need, s));
-    DDParams *p = new DDParams();
-    p->nx = g->nx; p->ny = g->ny; p->nz = g->nz; p->na = g->na; p->nb = g->nb;
-    p->cyl = g->det_kind == NEFCT_DET_CYL;
-    p->sid = g->src_det; p->sad = g->src_iso;
-    p->da = g->da; p->ai = g->a_offset; p->db = g->db; p->bi = g->b_offset;
-    p->proj = proj;
-    p->acc = (float *)ws;
-    const int cols = 4;
-    const int kMax = ViewTable<float>::kMax;
-    for (int v0 = 0; v0 < g->nv; v0 += kMax) {
-        const int nvc = std::min(kMax, g->nv - v0);
-        p->v0 = v0;
-        p->nvc = nvc;
-        for (int i = 0; i < nvc; ++i) {
-            const double a = (double)g->angles[v0 + i];
-            p->tab.cs[i] = (float)cos(a);
-            p->tab.sn[i] = (float)sin(a);
-            p->tab.off[i] = g->z_offsets ? g->z_offsets[v0 + i] : 0.f;
-        }
-        dim3 grid((g->na + cols - 1) / cols, (g->nb + 31) / 32, nvc);
-        dd_backproject_kernel<<<grid, dim3(32, cols), 0, s>>>(*p);
-        const cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) { delete p; return cuda_fail(e, "dd_backproject_kernel"); }
-    }
-    delete p;
-    const nefct_grid gr{g->nx, g->ny, g->nz, 0.f, 0.f, 0.f, (float)g->nx, (float)g->ny, (float)g->nz};
-    return zfold((const float *)ws, vol, gr, s);
+    return dd_impl<float>(g, proj, vol, 0, ws, ws_bytes, (cudaStream_t)stream, false);
+}
+
+nefct_status nefct_dd_forward(const nefct_dd_geom *g, const float *vol, float *proj, uint32_t flags, void *ws,
+                              size_t ws_bytes, void *stream)
+{
+    return dd_impl<float>(g, vol, proj, flags, ws, ws_bytes, (cudaStream_t)stream, true);
+}
+
+nefct_status nefct_dd_backward(const nefct_dd_geom *g, const float *proj, float *vol, uint32_t flags, void *ws,
+                               size_t ws_bytes, void *stream)
+{
+    return dd_impl<float>(g, proj, vol, flags, ws, ws_bytes, (cudaStream_t)stream, false);
+}
+
+nefct_status nefct_dd_forward_f64(const nefct_dd_geom *g, const double *vol, double *proj, uint32_t flags,
+                                  void *stream)
+{
+    return dd_impl<double>(g, vol, proj, flags, nullptr, 0, (cudaStream_t)stream, true);
+}
+
+nefct_status nefct_dd_backward_f64(const nefct_dd_geom *g, const double *proj, double *vol, uint32_t flags,
+                                   void *stream)
+{
+    return dd_impl<double>(g, proj, vol, flags, nullptr, 0, (cudaStream_t)stream, false);
 }
 
 }  // extern "C"

@@ -26,7 +26,8 @@ from ._lib import NefctError
 
 __all__ = ["ConeBeam", "cb_forward", "cb_backward", "cb_count_intersections", "lor_forward",
            "lor_backward", "fdk_filter", "fdk_backproject", "warp_forward", "warp_adjoint",
-           "warp_grad_dvf", "warp_invert", "project", "backproject", "warp", "NefctError"]
+           "warp_grad_dvf", "warp_invert", "project", "backproject", "warp", "DDGeometry", "dd_forward",
+           "dd_backward", "dd_backproject", "dd_project", "parker_direction", "NefctError"]
 
 
 @dataclass(eq=False)
@@ -353,6 +354,83 @@ def warp_invert(mx, my, mz, iters: int = 30):
     return ix, iy, iz
 
 
+class DDGeometry:
+    """Geometry of the distance-driven pair (dist_3d_back_fdk.cu.cc's
+    conventions): voxel units with the grid centred on the rotation axis;
+    shape (nx, ny, nz); src_iso = source-axis (the reference's SAD), src_det
+    = source-detector (its SID); bin ia at (ia + 0.5) * da + a_offset -
+    na * da / 2 (radians for a cylindrical detector), rows likewise; per-view
+    z offsets (None = 0)."""
+
+    def __init__(self, shape, angles, src_iso, src_det, na, da, nb, db, a_offset=0.0, b_offset=0.0,
+                 det_kind="flat", z_offsets=None):
+        self.shape = tuple(int(v) for v in shape)
+        self.angles = np.ascontiguousarray(np.asarray(angles, np.float32).reshape(-1))
+        self.z_offsets = None if z_offsets is None else np.ascontiguousarray(
+            np.asarray(z_offsets, np.float32).reshape(-1))
+        if self.z_offsets is not None and self.z_offsets.size != self.angles.size:
+            raise NefctError(_lib.ERR_INVALID, f"{self.z_offsets.size} z offsets for {self.angles.size} views")
+        self.src_iso, self.src_det = float(src_iso), float(src_det)
+        self.na, self.da, self.nb, self.db = int(na), float(da), int(nb), float(db)
+        self.a_offset, self.b_offset = float(a_offset), float(b_offset)
+        self.det_kind = det_kind
+
+    @property
+    def nv(self) -> int:
+        return int(self.angles.size)
+
+    @property
+    def vol_shape(self) -> tuple:
+        nx, ny, nz = self.shape
+        return (nz, ny, nx)
+
+    @property
+    def proj_shape(self) -> tuple:
+        return (self.nv, self.nb, self.na)
+
+    def struct(self) -> _lib.DDGeom:
+        nx, ny, nz = self.shape
+        return _lib.DDGeom(nx, ny, nz, self.nv, self.angles.ctypes.data_as(C.POINTER(C.c_float)),
+                           self.z_offsets.ctypes.data_as(C.POINTER(C.c_float)) if self.z_offsets is not None
+                           else None, self.src_iso, self.src_det, self.na, self.da, self.a_offset, self.nb, self.db,
+                           self.b_offset, _lib.DET_CYL if self.det_kind == "cyl" else _lib.DET_FLAT)
+
+
+def _dd_call(name: str, src: torch.Tensor, geom: DDGeometry, flags: int, out_shape: tuple) -> torch.Tensor:
+    if not isinstance(src, torch.Tensor) or not src.is_cuda:
+        raise NefctError(_lib.ERR_INVALID, f"{name} needs a CUDA tensor (there is no CPU path)")
+    if src.dtype not in (torch.float32, torch.float64):
+        raise NefctError(_lib.ERR_INVALID, f"{name} takes float32 or float64, got {src.dtype}")
+    src = src.contiguous()
+    out = torch.empty(out_shape, dtype=src.dtype, device=src.device)
+    g = geom.struct()
+    with torch.cuda.device(src.device):
+        if src.dtype == torch.float64:
+            _lib.call(f"nefct_dd_{name}_f64", C.byref(g), src.data_ptr(), out.data_ptr(), flags, _stream(src))
+        else:
+            wn = _lib.load().nefct_dd_workspace_bytes(C.byref(g))
+            ws = torch.empty(wn, dtype=torch.uint8, device=src.device)
+            _lib.call(f"nefct_dd_{name}", C.byref(g), src.data_ptr(), out.data_ptr(), flags, ws.data_ptr(), wn,
+                      _stream(src))
+    return out
+
+
+def dd_forward(vol: torch.Tensor, geom: DDGeometry, flags: int = 0) -> torch.Tensor:
+    """Distance-driven forward projection [nz][ny][nx] -> [nv][nb][na]: the
+    exact transpose of dd_backward with the same flags (flags 0: with the FDK
+    weight, the transpose of the reference's FDK backprojection;
+    FDK_NO_WEIGHT: footprint-weighted line integrals)."""
+    _check_tensor(vol, geom.vol_shape, "vol")
+    return _dd_call("forward", vol, geom, flags, geom.proj_shape)
+
+
+def dd_backward(proj: torch.Tensor, geom: DDGeometry, flags: int = 0) -> torch.Tensor:
+    """Distance-driven backprojection [nv][nb][na] -> [nz][ny][nx] (flags 0:
+    dist_3d_back_fdk's FDK-weighted backprojection)."""
+    _check_tensor(proj, geom.proj_shape, "proj")
+    return _dd_call("backward", proj, geom, flags, geom.vol_shape)
+
+
 def dd_backproject(proj, shape, angles, src_iso: float, src_det: float, da: float, db: float,
                    a_offset: float = 0.0, b_offset: float = 0.0, det_kind: str = "flat", z_offsets=None):
     """Distance-driven FDK-weighted backprojection (back_project_{flat,cyli}_fdk_gpu,
@@ -362,24 +440,19 @@ def dd_backproject(proj, shape, angles, src_iso: float, src_det: float, da: floa
     voxel units with the grid centred on the axis; src_iso = source-axis
     (the reference's SAD), src_det = source-detector (its SID); bin ia sits at
     (ia + 0.5) * da + a_offset - na * da / 2.  Returns [nz][ny][nx]."""
-    if not proj.is_cuda:
+    if not isinstance(proj, torch.Tensor) or not proj.is_cuda:
         raise NefctError(_lib.ERR_INVALID, "dd_backproject needs a CUDA tensor (there is no CPU path)")
     if proj.dtype != torch.float32 or proj.dim() != 3:
         raise NefctError(_lib.ERR_INVALID, "proj must be float32 [nv][nb][na]")
     proj = proj.contiguous()
     nv, nb, na = proj.shape
-    ang = np.ascontiguousarray(np.asarray(angles, np.float32).reshape(-1))
-    if ang.size != nv:
-        raise NefctError(_lib.ERR_INVALID, f"{ang.size} angles for {nv} views")
-    off = None if z_offsets is None else np.ascontiguousarray(np.asarray(z_offsets, np.float32).reshape(-1))
-    nx, ny, nz = (int(v) for v in shape)
-    g = _lib.DDGeom(nx, ny, nz, nv, ang.ctypes.data_as(C.POINTER(C.c_float)),
-                    off.ctypes.data_as(C.POINTER(C.c_float)) if off is not None else None,
-                    float(src_iso), float(src_det), na, float(da), float(a_offset), nb, float(db), float(b_offset),
-                    _lib.DET_CYL if det_kind == "cyl" else _lib.DET_FLAT)
+    geom = DDGeometry(shape, angles, src_iso, src_det, na, da, nb, db, a_offset, b_offset, det_kind, z_offsets)
+    if geom.nv != nv:
+        raise NefctError(_lib.ERR_INVALID, f"{geom.nv} angles for {nv} views")
+    out = torch.empty(geom.vol_shape, dtype=torch.float32, device=proj.device)
+    g = geom.struct()
     wn = _lib.load().nefct_dd_workspace_bytes(C.byref(g))
     ws = torch.empty(wn, dtype=torch.uint8, device=proj.device)
-    out = torch.empty((nz, ny, nx), dtype=torch.float32, device=proj.device)
     with torch.cuda.device(proj.device):
         _lib.call("nefct_dd_backproject", C.byref(g), proj.data_ptr(), out.data_ptr(), ws.data_ptr(), wn,
                   _stream(proj))
@@ -428,6 +501,23 @@ class _Warp(torch.autograd.Function):
         if any(ctx.needs_input_grad[1:]):
             gx, gy, gz = warp_grad_dvf(img, mx, my, mz, g)
         return gi, gx, gy, gz
+
+
+class _DDProject(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, vol, geom, flags):
+        ctx.geom, ctx.flags = geom, flags
+        return dd_forward(vol.contiguous(), geom, flags)
+
+    @staticmethod
+    def backward(ctx, g):
+        return dd_backward(g.contiguous(), ctx.geom, ctx.flags), None, None
+
+
+def dd_project(vol: torch.Tensor, geom: DDGeometry, flags: int = 0) -> torch.Tensor:
+    """Differentiable distance-driven forward projection (backward = the
+    hand-written exact transpose, dd_backward with the same flags)."""
+    return _DDProject.apply(vol, geom, flags)
 
 
 def project(vol: torch.Tensor, geom: ConeBeam, flags: int = _lib.REF_FORWARD) -> torch.Tensor:

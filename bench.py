@@ -643,72 +643,136 @@ def uneven_geoms(n_problems=64, seed=4, scale=1.0, view_scale=1.0):
     return geoms
 
 
+def small_geoms(n_problems=96, seed=44):
+    """Many small uneven problems (a minibatch of small reconstructions):
+    edge log-uniform in [16, 64], views U{8..64}, detector rows/cols
+    U{24..128}, the same scanner distribution as uneven_geoms."""
+    import nefct_b200 as nb
+    rng = np.random.default_rng(seed)
+    geoms = []
+    for _ in range(n_problems):
+        n = int(round(np.exp(rng.uniform(np.log(16), np.log(64)))))
+        nv = int(rng.integers(8, 65))
+        rows, cols = (int(v) for v in rng.integers(24, 129, 2))
+        si = float(rng.uniform(400, 700))
+        sd = si * float(rng.uniform(1.5, 2.0))
+        pixel = (sd / si) * n * 1.0 / cols
+        ang = np.linspace(0, 2 * np.pi, nv, endpoint=False).astype(np.float32)
+        geoms.append(nb.ConeBeam((n, n, n), ang, si, sd, cols, pixel, rows, pixel, size=(float(n),) * 3))
+    return geoms
+
+
 def run_batched(args):
-    """Batched fwd+adjoint iterations/s of the uneven problems vs the plain
-    per-problem drop-in path (numpy in/out per call, like the reference's
-    operators) and vs sequential per-problem device calls."""
+    """Batched fwd+adjoint iterations/s of uneven problems: the batch plan
+    replayed as a CUDA graph, and one autograd iteration through
+    batch_project (loss sum_i ||A_i x_i||^2 / 2, backward = one batched
+    transpose), against sequential per-problem device calls (plain and
+    through autograd) and the plain per-problem drop-in path (numpy in/out
+    per call, like the reference's operators; warmed up first)."""
     import torch
     import nefct_b200 as nb
     from nefct_b200 import ops
-    from nefct_b200.batch import BatchProjector
+    from nefct_b200.batch import BatchProjector, batch_project
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    geoms = uneven_geoms(args.problems, 4, args.scale, args.view_scale)
+    if args.regime == "small":
+        geoms = small_geoms(args.problems if args.problems else 96)
+        workload = (f"{len(geoms)} small problems, edge log-U[16,64], views U[8,64], detector U[24,128]^2, "
+                    f"seed 44")
+    else:
+        geoms = uneven_geoms(args.problems if args.problems else 64, 4, args.scale, args.view_scale)
+        workload = (f"{len(geoms)} problems, edge log-U[64,384]x{args.scale}, views U[60,720]x{args.view_scale}, "
+                    f"detector U[128,1024]^2 x{args.scale}, seed 4")
     gen = torch.Generator(device=dev).manual_seed(4)
     vols = [torch.rand(g.vol_shape, device=dev, generator=gen) for g in geoms]
     bp = BatchProjector(geoms, vols)            # grads = the forward outputs (loss = |Ax|^2 / 2)
     inter = sum(ops.cb_count_intersections(g, 0, dev) for g in geoms)
+
+    def timed(fn, reps):
+        for _ in range(max(1, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / reps
+
     graph = bp.capture()
-    for _ in range(args.warmup):
-        graph.replay()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(args.steps):
-        graph.replay()
-    e1.record()
-    torch.cuda.synchronize()
-    t_batch = e0.elapsed_time(e1) / 1e3 / args.steps
+    t_batch = timed(graph.replay, args.steps)
+    strategies = {}
+    for name in ("persistent", "per-problem"):
+        bp.set_strategy(name)
+        g2 = bp.capture()
+        strategies[name] = 1e3 * timed(g2.replay, args.steps)
+        del g2
+    best = min(strategies, key=strategies.get)
+    bp.set_strategy(best)
+
+    # one autograd iteration through the batched Function
+    xs = [v.clone().requires_grad_() for v in vols]
+    grads_bp = BatchProjector(geoms, [v.detach().clone() for v in vols],
+                              grads=[torch.empty(g.sino_shape, device=dev) for g in geoms], strategy=best)
+
+    def autograd_batched():
+        for x in xs:
+            x.grad = None
+        sinos = batch_project(grads_bp, xs)
+        (sum((s * s).sum() for s in sinos) / 2).backward()
+    t_autograd = timed(autograd_batched, args.steps)
 
     # sequential per-problem device calls (the same kernels, one problem at a time)
-    for g, v, s_, b in zip(geoms, vols, bp.sinos, bp.backs):      # warm the allocator's workspaces
-        ops.cb_forward(v, g, 0, out=s_)
-        ops.cb_backward(s_, g, 0, out=b)
-    torch.cuda.synchronize()
-    e0.record()
-    for g, v, s_, b in zip(geoms, vols, bp.sinos, bp.backs):
-        ops.cb_forward(v, g, 0, out=s_)
-        ops.cb_backward(s_, g, 0, out=b)
-    e1.record()
-    torch.cuda.synchronize()
-    t_seq = e0.elapsed_time(e1) / 1e3
+    sinos = [torch.empty(g.sino_shape, device=dev) for g in geoms]
+    backs = [torch.empty(g.vol_shape, device=dev) for g in geoms]
+
+    def sequential():
+        for g, v, s_, b in zip(geoms, vols, sinos, backs):
+            ops.cb_forward(v, g, 0, out=s_)
+            ops.cb_backward(s_, g, 0, out=b)
+    t_seq = timed(sequential, max(1, args.steps // 2))
+
+    def sequential_autograd():
+        for g, x in zip(geoms, xs):
+            x.grad = None
+            s_ = nb.project(x, g)
+            ((s_ * s_).sum() / 2).backward()
+    t_seq_ag = timed(sequential_autograd, max(1, args.steps // 2))
 
     # plain drop-in path: numpy volume in, Project3D, BackProject3D, numpy out
     sc = [nb.ScannerConfig3D("flat", g.src_det, g.src_iso, nb.DetectorDirectAConfig(g.na, g.na * g.da),
                              nb.DetectorDirectBConfig(g.nb, g.nb * g.db)) for g in geoms]
     host = [v.permute(2, 1, 0).cpu().numpy() for v in vols]
+
+    def plain(idx):
+        for i in idx:
+            g = geoms[i]
+            img = nb.Image3D(host[i], [0, 0, 0], list(g.size))
+            proj = nb.Project3D(sc[i], g.angles, None)(img)
+            nb.BackProject3D(sc[i], list(g.shape), 1.0, "transpose")(proj)
+        torch.cuda.synchronize()
+    plain(range(min(4, len(geoms))))                 # warm-up (first calls, allocator growth)
     t0 = time.perf_counter()
-    for g, c, h in zip(geoms, sc, host):
-        img = nb.Image3D(h, [0, 0, 0], list(g.size))
-        proj = nb.Project3D(c, g.angles, None)(img)
-        nb.BackProject3D(c, list(g.shape), 1.0, "transpose")(proj)
-    torch.cuda.synchronize()
+    plain(range(len(geoms)))
     t_plain = time.perf_counter() - t0
-    line = {"metric": "batched fwd+adjoint iterations/s (64 uneven cone-beam problems)", "value": 1.0 / t_batch,
-            "unit": "iterations/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * t_batch, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic (seeded uniform random volumes)",
-            "config": {"workload": f"{args.problems} problems, edge log-U[64,384]x{args.scale}, "
-                                   f"views U[60,720]x{args.view_scale}, "
-                                   f"detector U[128,1024]^2 x{args.scale}, seed 4",
-                       "voxels": int(sum(np.prod(g.shape) for g in geoms)),
+    line = {"metric": "batched autograd fwd+adjoint iterations/s (uneven cone-beam problems)",
+            "value": 1.0 / t_autograd, "unit": "iterations/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_autograd, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded uniform random volumes)",
+            "config": {"workload": workload, "voxels": int(sum(np.prod(g.shape) for g in geoms)),
                        "rays": int(sum(g.nv * g.na * g.nb for g in geoms)), "tiles": bp.tiles},
-            "extras": {"strategy": bp.strategy, "strategy_step_ms": bp.timings,
+            "extras": {"strategy": best, "graph_replay_ms_by_strategy": strategies,
                        "intersections_per_iteration": 2 * inter,
-                       "batched_intersections_per_s": 2 * inter / t_batch,
-                       "sequential_device_s": t_seq, "plain_dropin_s": t_plain,
-                       "speedup_vs_plain_dropin": t_plain / t_batch,
-                       "speedup_vs_sequential_device": t_seq / t_batch}}
+                       "batched_graph_replay_ms": 1e3 * t_batch,
+                       "batched_autograd_ms": 1e3 * t_autograd,
+                       "batched_autograd_intersections_per_s": 2 * inter / t_autograd,
+                       "sequential_device_ms": 1e3 * t_seq, "sequential_device_autograd_ms": 1e3 * t_seq_ag,
+                       "plain_dropin_ms": 1e3 * t_plain,
+                       "speedup_vs_plain_dropin": t_plain / t_autograd,
+                       "speedup_vs_sequential_device": t_seq / t_autograd,
+                       "speedup_vs_sequential_device_autograd": t_seq_ag / t_autograd,
+                       "graph_replay_speedup_vs_sequential_device": t_seq / t_batch}}
     print(json.dumps(line), flush=True)
 
 
@@ -959,7 +1023,9 @@ def main():
     ap.add_argument("--order", type=int, default=0, help="with --rows: 0 row bands outermost, 1 views outermost")
     ap.add_argument("--walk", type=int, default=3,
                     help="with --rows: column warps for the forward (bit 0) / adjoint (bit 1), else thread per ray")
-    ap.add_argument("--problems", type=int, default=64)
+    ap.add_argument("--problems", type=int, default=0, help="batched: problem count (0 = the regime's)")
+    ap.add_argument("--regime", default="uneven", choices=["uneven", "small"],
+                    help="batched: the 64 uneven problems (edges 64..384) or 96 small ones (edges 16..64)")
     ap.add_argument("--scale", type=float, default=1.0, help="batched: scale of volume edges and detector sizes")
     ap.add_argument("--view-scale", type=float, default=1.0, help="batched: scale of the view counts")
     args = ap.parse_args()

@@ -4,6 +4,7 @@ optionally replayed as a CUDA graph (include/nefct_b200.h, nefct_cb_batch_*).
     bp = BatchProjector(geoms, vols)          # plans, allocates, binds
     bp.step()                                 # forward of all, then transpose of all
     g = bp.capture()                          # CUDA graph of one step; g.replay()
+    sinos = bp.project(vols)                  # autograd: backward runs the batched transpose
 
 Per problem i: ``sinos[i] = A_i vols[i]`` and ``backs[i] = A_i^T grads[i]``
 (``grads`` defaults to ``sinos``).  Forward outputs are bitwise equal to
@@ -17,7 +18,47 @@ import torch
 
 from . import _lib, ops
 
-__all__ = ["BatchProjector"]
+__all__ = ["BatchProjector", "batch_project"]
+
+
+class _BatchProject(torch.autograd.Function):
+    """Forward: the plan's batched forward of every problem; backward: the
+    plan's batched exact transpose of the incoming gradients.  Volumes that
+    are not the plan's own bound tensors are copied into them first; the
+    returned sinograms are the plan's bound output tensors (no copy), valid
+    until the plan's next forward."""
+
+    @staticmethod
+    def forward(ctx, bp, *vols):
+        for v, dst in zip(vols, bp.vols):
+            if v.data_ptr() != dst.data_ptr():
+                dst.copy_(v)
+        bp.forward()
+        ctx.bp = bp
+        return tuple(bp.sinos)
+
+    @staticmethod
+    def backward(ctx, *grads):
+        bp = ctx.bp
+        for g, dst in zip(grads, bp.grads):
+            if g is None:
+                dst.zero_()
+            elif g.data_ptr() != dst.data_ptr():
+                dst.copy_(g)
+        bp.backward()
+        return (None, *bp.backs)
+
+
+def batch_project(bp: "BatchProjector", vols: list) -> tuple:
+    """Differentiable batched forward projection of vols (one per problem of
+    the plan); d(loss)/d(vols[i]) = A_i^T d(loss)/d(sinos[i]), computed by
+    one batched transpose."""
+    if len(vols) != len(bp.vols):
+        raise _lib.NefctError(_lib.ERR_INVALID, f"{len(vols)} volumes for a plan of {len(bp.vols)} problems")
+    for v, g in zip(vols, bp.geoms):
+        if tuple(v.shape) != g.vol_shape or v.dtype != torch.float32 or v.device != bp.device:
+            raise _lib.NefctError(_lib.ERR_INVALID, "volumes must match the plan (float32 [nz, ny, nx], its device)")
+    return _BatchProject.apply(bp, *vols)
 
 
 class BatchProjector:
@@ -92,6 +133,10 @@ class BatchProjector:
     def step(self):
         self.forward()
         self.backward()
+
+    def project(self, vols: list) -> tuple:
+        """batch_project(self, vols): differentiable batched forward."""
+        return batch_project(self, vols)
 
     def capture(self) -> torch.cuda.CUDAGraph:
         """CUDA graph of one step (forward of all problems, then transpose of all)."""

@@ -57,6 +57,35 @@ def test_pixel_backprojection_vs_reference_fixtures(cuda, golden):
         assert_parity(out, golden[key])
 
 
+@pytest.mark.skipif("not __import__('oracle').have_ref()")
+@pytest.mark.parametrize("phi", [0.0, 0.7, 2.9])
+def test_fdk_distance_weight_pinned_by_reference_kernel(cuda, oracle_lib, phi):
+    """The FDK distance weight src_iso^2 / (src_iso + x cos + y sin)^2
+    (backprojection.m:11-12) is pinned against the reference's own kernel
+    that applies it, dist_3d_back_fdk.cu.cc:153-154 (built for the host):
+    for one view of an all-ones projection, that kernel's output divided by
+    this library's weight-free distance-driven backprojection (same
+    footprints and fractions) is the reference's weight per voxel; the
+    voxel-driven FDK backprojection's weighted / unweighted ratio must
+    equal it (1 mm voxels, grid centred on the axis, even sizes so both
+    place voxel centres at (i + 0.5 - n / 2))."""
+    n, na, nbr, sid, sdd = 32, 96, 80, 60.0, 120.0
+    ang = np.array([phi], np.float32)
+    ones = np.ones((1, nbr, na), np.float32)
+    dg = ops.DDGeometry((n, n, n), ang, sid, sdd, na, 1.0, nbr, 1.0)
+    ref_w = oracle_lib.ref_dd_backproject(ones, ang, (n, n, n), sdd, sid, na, 1.0, 0.0, nbr, 1.0, 0.0)
+    ours_nw = ops.dd_backward(torch.from_numpy(ones).to(cuda), dg, nb._lib.FDK_NO_WEIGHT).cpu().numpy()
+    g = nb.ConeBeam((n, n, n), ang, sid, sdd, na, 1.0, nbr, 1.0, size=(float(n),) * 3)
+    t = torch.from_numpy(ones).to(cuda)
+    fw = ops.fdk_backproject(t, g, weight=True).cpu().numpy()
+    fnw = ops.fdk_backproject(t, g, weight=False).cpu().numpy()
+    inside = (ours_nw > 1e-3 * ours_nw.max()) & (fnw > 0.5)
+    assert inside.sum() > 0.3 * n ** 3
+    w_ref = ref_w[inside] / ours_nw[inside]
+    w_ours = fw[inside] / fnw[inside]
+    np.testing.assert_allclose(w_ours, w_ref, rtol=5e-6)
+
+
 def test_weighted_backprojection_vs_oracle(cuda, oracle_lib):
     ang = np.linspace(0, 2 * np.pi, 50, endpoint=False).astype(np.float32)
     g = nb.ConeBeam((30, 26, 22), ang, 250.0, 500.0, 64, 1.7, 48, 1.4, center=(1.0, -2.0, 0.5),

@@ -322,9 +322,8 @@ def run_gpu(args):
     ceil = measure_ceilings(dev)
 
     if args.rows:
-        autotune.apply(args.rows, args.order, args.walk, args.combine)   # fixed launch shape (profiling)
-        tuned = {"rows": args.rows, "order": args.order, "walk": args.walk, "combine": args.combine, "ms": None,
-                 "views": None}
+        autotune.apply(args.rows, args.order, args.walk)               # fixed launch shape (profiling)
+        tuned = {"rows": args.rows, "order": args.order, "walk": args.walk, "ms": None, "views": None}
     else:
         # untimed launch-shape choice on every tune_every-th view of the scan
         sub = geom.subset(np.arange(0, c["nv"], c["tune_every"]))
@@ -463,7 +462,6 @@ def run_gpu(args):
                                "grid_order": "row-band outermost" if tuned["order"] == 0 else "view outermost",
                                "walk": {"forward": "column warps" if walk & 1 else "thread per ray",
                                         "adjoint": "column warps" if walk & 2 else "thread per ray"},
-                               "adjoint_run_combining": bool(tuned.get("combine")),
                                "tuned_on_views": tuned.get("views"), "autotune_ms": tuned["ms"]}}
 
     # parity and CPU baseline: the reference's host build on sampled views
@@ -472,7 +470,7 @@ def run_gpu(args):
     if rank == 0 and ws == 1 and "parity" in legs:
         cpu, extras["parity"] = parity_and_baseline(c, geom, vol, dev)
 
-    if "extras" in legs and rank == 0:
+    if "extras" in legs and rank == 0 and ws == 1:
         extras.update(other_scans(c, dev, with_cpu="parity" in legs))
 
     if rank == 0:
@@ -1025,8 +1023,6 @@ def main():
     ap.add_argument("--order", type=int, default=0, help="with --rows: 0 row bands outermost, 1 views outermost")
     ap.add_argument("--walk", type=int, default=3,
                     help="with --rows: column warps for the forward (bit 0) / adjoint (bit 1), else thread per ray")
-    ap.add_argument("--combine", type=int, default=0,
-                    help="with --rows: 1 = the column-warp adjoint sums neighbouring rows on one voxel first")
     ap.add_argument("--problems", type=int, default=0, help="batched: problem count (0 = the regime's)")
     ap.add_argument("--regime", default="uneven", choices=["uneven", "small"],
                     help="batched: the 64 uneven problems (edges 64..384) or 96 small ones (edges 16..64)")

@@ -55,19 +55,11 @@ const char *nefct_last_error(void);
  *                        rows of one detector column, which share their
  *                        transverse walk, over a z-fastest copy of the volume,
  *                        and NEFCT_TUNE_CB_ROWS counts columns per CTA; a
- *                        clear bit: one thread per ray.  Default 3
- *   NEFCT_TUNE_CB_COMBINE 1: the column-warp transpose first sums, per slab,
- *                        the contributions of neighbouring rows (lanes) that
- *                        fall on the same voxel and issues one reduction per
- *                        run of them (worth it where rows are closer than a
- *                        voxel at the volume); 0: one reduction per
- *                        contribution.  Same contributions either way; only
- *                        the float summation order differs.  Default 0 */
-#define NEFCT_TUNE_CB_ROWS    0
-#define NEFCT_TUNE_CB_ORDER   1
-#define NEFCT_TUNE_CB_WALK    2
-#define NEFCT_TUNE_CB_COMBINE 3
-#define NEFCT_TUNE_COUNT      4
+ *                        clear bit: one thread per ray.  Default 3 */
+#define NEFCT_TUNE_CB_ROWS  0
+#define NEFCT_TUNE_CB_ORDER 1
+#define NEFCT_TUNE_CB_WALK  2
+#define NEFCT_TUNE_COUNT    3
 nefct_status nefct_tune_set(int32_t key, int32_t value);
 int32_t nefct_tune_get(int32_t key);
 

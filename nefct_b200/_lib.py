@@ -31,7 +31,7 @@ LOR_REF_BACKPROJECT = TIE_GT | SKIP_SHORT | NO_INV_L2
 FDK_NO_WEIGHT = 0x100
 
 DET_FLAT, DET_CYL = 0, 1
-TUNE_CB_ROWS, TUNE_CB_ORDER, TUNE_CB_WALK, TUNE_CB_COMBINE = 0, 1, 2, 3
+TUNE_CB_ROWS, TUNE_CB_ORDER, TUNE_CB_WALK = 0, 1, 2
 BATCH_PERSISTENT, BATCH_PER_PROBLEM = 0, 1
 WIN_RAM_LAK, WIN_SHEPP_LOGAN, WIN_COSINE, WIN_HAMMING, WIN_HANN = 0, 1, 2, 3, 4
 WINDOWS = {"ram-lak": WIN_RAM_LAK, "shepp-logan": WIN_SHEPP_LOGAN, "cosine": WIN_COSINE,

@@ -3,8 +3,7 @@
 For a geometry signature (grid, views, detector, kind, flags) it times the
 equivalent launch variants of include/nefct_b200.h's tuning table -- the walk
 (one thread per ray, or one warp per 32 rows of a detector column), rows or
-columns per CTA, the grid order and, for the column-warp transpose, run
-combining (NEFCT_TUNE_CB_COMBINE) -- on the current device with CUDA
+columns per CTA and the grid order -- on the current device with CUDA
 events (forward + transpose, after a warm-up), applies the fastest with
 nefct_tune_set and caches the choice in a JSON file
 (``$NEFCT_TUNE_CACHE``, default ``~/.cache/nefct_b200/tune.json``).  Every
@@ -60,19 +59,17 @@ def _store(db: dict) -> None:
         pass
 
 
-def apply(rows: int, order: int, walk: int | None = None, combine: int | None = None) -> None:
+def apply(rows: int, order: int, walk: int | None = None) -> None:
     _lib.call("nefct_tune_set", _lib.TUNE_CB_ROWS, int(rows))
     _lib.call("nefct_tune_set", _lib.TUNE_CB_ORDER, int(order))
     if walk is not None:
         _lib.call("nefct_tune_set", _lib.TUNE_CB_WALK, int(walk))
-    if combine is not None:
-        _lib.call("nefct_tune_set", _lib.TUNE_CB_COMBINE, int(combine))
 
 
 def current() -> dict:
     lib = _lib.load()
     return {"rows": lib.nefct_tune_get(_lib.TUNE_CB_ROWS), "order": lib.nefct_tune_get(_lib.TUNE_CB_ORDER),
-            "walk": lib.nefct_tune_get(_lib.TUNE_CB_WALK), "combine": lib.nefct_tune_get(_lib.TUNE_CB_COMBINE)}
+            "walk": lib.nefct_tune_get(_lib.TUNE_CB_WALK)}
 
 
 def tune_cone_beam(geom: ops.ConeBeam, flags: int = 0, device=None, reps: int = 2, use_cache: bool = True) -> dict:
@@ -82,8 +79,8 @@ def tune_cone_beam(geom: ops.ConeBeam, flags: int = 0, device=None, reps: int = 
     key = signature(geom, flags, device)
     with _lock:
         db = _load() if use_cache else {}
-        if key in db and "combine" in db[key]:
-            apply(db[key]["rows"], db[key]["order"], db[key]["walk"], db[key]["combine"])
+        if key in db and "walk" in db[key]:
+            apply(db[key]["rows"], db[key]["order"], db[key]["walk"])
             return db[key]
         gen = torch.Generator(device=device).manual_seed(0)
         vol = torch.rand(geom.vol_shape, device=device, generator=gen)
@@ -91,42 +88,35 @@ def tune_cone_beam(geom: ops.ConeBeam, flags: int = 0, device=None, reps: int = 
         sino = torch.empty(geom.sino_shape, device=device)
         back = torch.empty(geom.vol_shape, device=device)
         # forward and transpose are timed separately for each walk; rows and
-        # order are shared, the walk is chosen per direction, and the
-        # column-warp transpose with and without run combining
+        # order are shared, the walk is chosen per direction
         times, best = {}, None
         for rows in _ROWS:
             for order in _ORDERS:
                 t_dir = {}
                 for walk in _WALKS:
                     apply(rows, order, 3 * walk)
-                    for name, fn, combos in (("fwd", lambda: ops.cb_forward(vol, geom, flags, out=sino), (0,)),
-                                             ("bwd", lambda: ops.cb_backward(grad, geom, flags, out=back),
-                                              (0, 1) if walk else (0,))):
-                        for cmb in combos:
-                            apply(rows, order, 3 * walk, cmb)
+                    for name, fn in (("fwd", lambda: ops.cb_forward(vol, geom, flags, out=sino)),
+                                     ("bwd", lambda: ops.cb_backward(grad, geom, flags, out=back))):
+                        fn()
+                        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                        e0.record()
+                        for _ in range(reps):
                             fn()
-                            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                            e0.record()
-                            for _ in range(reps):
-                                fn()
-                            e1.record()
-                            e1.synchronize()
-                            t_dir[(name, walk, cmb)] = e0.elapsed_time(e1) / reps
-                wf = min(_WALKS, key=lambda w: t_dir[("fwd", w, 0)])
-                wb, cb = min(((w, c) for (d, w, c) in t_dir if d == "bwd"), key=lambda k: t_dir[("bwd",) + k])
+                        e1.record()
+                        e1.synchronize()
+                        t_dir[(name, walk)] = e0.elapsed_time(e1) / reps
+                wf = min(_WALKS, key=lambda w: t_dir[("fwd", w)])
+                wb = min(_WALKS, key=lambda w: t_dir[("bwd", w)])
                 for walk in _WALKS:
-                    bwd = min(t for (d, w, c), t in t_dir.items() if d == "bwd" and w == walk)
-                    times[f"{rows}/{order}/{3 * walk}"] = t_dir[("fwd", walk, 0)] + bwd
-                    times[f"{rows}/{order}/{3 * walk}/fwd"] = t_dir[("fwd", walk, 0)]
-                    times[f"{rows}/{order}/{3 * walk}/bwd"] = bwd
-                    if walk:
-                        times[f"{rows}/{order}/{3 * walk}/bwd/combine"] = t_dir[("bwd", walk, 1)]
-                total = t_dir[("fwd", wf, 0)] + t_dir[("bwd", wb, cb)]
+                    times[f"{rows}/{order}/{3 * walk}"] = t_dir[("fwd", walk)] + t_dir[("bwd", walk)]
+                    times[f"{rows}/{order}/{3 * walk}/fwd"] = t_dir[("fwd", walk)]
+                    times[f"{rows}/{order}/{3 * walk}/bwd"] = t_dir[("bwd", walk)]
+                total = t_dir[("fwd", wf)] + t_dir[("bwd", wb)]
                 if best is None or total < best[0]:
-                    best = (total, rows, order, wf | (wb << 1), cb if wb else 0)
-        _, rows, order, walk, combine = best
-        apply(rows, order, walk, combine)
-        rec = {"rows": rows, "order": order, "walk": walk, "combine": combine, "ms": times}
+                    best = (total, rows, order, wf | (wb << 1))
+        _, rows, order, walk = best
+        apply(rows, order, walk)
+        rec = {"rows": rows, "order": order, "walk": walk, "ms": times}
         if use_cache:
             db = _load()
             db[key] = rec

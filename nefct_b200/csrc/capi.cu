@@ -12,7 +12,7 @@ static thread_local char g_last_error[512] = "";
 
 // Launch-shape knobs; every value runs the same per-ray arithmetic (the
 // forward's output does not depend on them).
-static std::atomic<int> g_tune[NEFCT_TUNE_COUNT] = {{8}, {0}, {3}, {0}};
+static std::atomic<int> g_tune[NEFCT_TUNE_COUNT] = {{8}, {0}, {3}};
 
 static bool tune_valid(int key, int value)
 {
@@ -20,7 +20,6 @@ static bool tune_valid(int key, int value)
     case NEFCT_TUNE_CB_ROWS: return value == 1 || value == 2 || value == 4 || value == 8;
     case NEFCT_TUNE_CB_ORDER: return value == 0 || value == 1;
     case NEFCT_TUNE_CB_WALK: return value >= 0 && value <= 3;
-    case NEFCT_TUNE_CB_COMBINE: return value == 0 || value == 1;
     default: return false;
     }
 }

@@ -91,47 +91,14 @@ __global__ void __launch_bounds__(256) cb_backward_kernel(const __grid_constant_
     ray_backward<T, DIV, EXACT>(p.g, r, p.flags, y, p.out, p.outT);
 }
 
-// Reduces slot i of every lane of the warp into acc, one reduction per run
-// of neighbouring lanes whose slot falls on the same voxel.  The slab's
-// voxel index grows with the row (lane) along a slot, so equal indices sit
-// in runs of adjacent lanes; each lane sums its run's values from its own
-// lane onward by doubling spans (lane l covers [l, l + span) and stays open
-// while the run continues past it), stopping when no lane is open, and the
-// run's first lane issues the reduction.  Inactive slots take a key no voxel
-// has and never reduce.  Whole warp, uniform control flow.
-template <int NS, bool CHK>
-__device__ __forceinline__ void red_runs(float *acc, const ColSlots<NS, CHK> &s, int i, float yw)
-{
-    const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    const bool ok = s.ok[i];
-    const unsigned key = ok ? s.idx[i] : 0xffffffffu;
-    float v = ok ? yw * s.r[i] : 0.f;
-    const unsigned knext = __shfl_down_sync(full, key, 1);
-    const unsigned kprev = __shfl_up_sync(full, key, 1);
-    const bool head = ok && (lane == 0 || kprev != key);
-    bool open = ok && lane < 31 && knext == key;
-#pragma unroll 1
-    for (int d = 1; d < 32 && __any_sync(full, open); d <<= 1) {
-        const float t = __shfl_down_sync(full, v, d);
-        const bool to = __shfl_down_sync(full, (int)open, d) != 0;
-        if (open) {
-            v += t;
-            open = to;
-        }
-    }
-    if (head) atomicAdd(acc + key, v);
-}
-
 // One lane of a column warp (the whole warp calls it together).  has: the
 // lane has a ray r; FWD: gathers from the z-fastest copy volZ into *out;
 // otherwise reduces y times the ray's weights into the z-fastest accumulator
-// accZ -- one reduction per contribution, or (COMBINE) one per run of
-// neighbouring lanes on the same voxel (red_runs) -- or (FIX) as 64-bit
-// fixed-point integers (value * weight * scale, rounded) into fixZ.  Rays
-// without a contribution (outside the detector, missing the grid, zero
-// value) stay in the warp's walk with every slot inactive.
-template <bool DIV, bool FWD, bool FIX = false, bool COMBINE = false>
+// accZ, or (FIX) as 64-bit fixed-point integers (value * weight * scale,
+// rounded) into fixZ.  Rays without a contribution (outside the detector,
+// missing the grid, zero value) stay in the warp's walk with every slot
+// inactive.
+template <bool DIV, bool FWD, bool FIX = false>
 __device__ __forceinline__ void colwarp_lane(const GridDev<float> &g, const float *r, bool has, uint32_t flags,
                                              const float *__restrict__ volZ, float *out, float y, float *accZ,
                                              unsigned long long *fixZ = nullptr, float scale = 0.f)
@@ -181,16 +148,6 @@ __device__ __forceinline__ void colwarp_lane(const GridDev<float> &g, const floa
                 if (s.ok[i]) atomicAdd(fixZ + s.idx[i], (unsigned long long)to_fixed((yw * s.r[i]) * scale));
         };
         col_walk_any<DIV, true>(c, L, K0, K1, KI0, KI1, g, f);
-    } else if constexpr (COMBINE) {
-        const float yw = y * w.W;
-        auto f = [&](const auto &s) {
-            red_runs(accZ, s, 0, yw);
-            // later slots are active in few lanes (a crossing in the slab)
-#pragma unroll
-            for (int i = 1; i < s.n; ++i)
-                if (__any_sync(0xffffffffu, s.ok[i])) red_runs(accZ, s, i, yw);
-        };
-        col_walk_any<DIV, true>(c, L, K0, K1, KI0, KI1, g, f);
     } else {
         const float yw = y * w.W;
         auto f = [&](const auto &s) {
@@ -206,7 +163,7 @@ __device__ __forceinline__ void colwarp_lane(const GridDev<float> &g, const floa
 // over the z-fastest copy p.volT (forward, into p.out) or accumulator p.outT.
 // (at most 64 registers: 4 CTAs of 256 threads per SM; measured faster than
 // the unconstrained 70)
-template <bool DIV, bool FWD, bool COMBINE = false>
+template <bool DIV, bool FWD>
 __global__ void __launch_bounds__(256, 4) cb_colwarp_kernel(const __grid_constant__ CBParams<float> p)
 {
     const int lane = threadIdx.x;
@@ -221,7 +178,7 @@ __global__ void __launch_bounds__(256, 4) cb_colwarp_kernel(const __grid_constan
     float r[6];
     cb_ray(p, ia, has ? ib : 0, iv, r);
     float *const out = FWD ? p.out + (size_t)(p.v0 + iv) * p.na * p.nb + (size_t)ib * p.na + ia : nullptr;
-    colwarp_lane<DIV, FWD, false, COMBINE>(p.g, r, has, p.flags, p.volT, out, y, p.outT);
+    colwarp_lane<DIV, FWD>(p.g, r, has, p.flags, p.volT, out, y, p.outT);
 }
 
 // Launch shape of the thread walk for nvc views (see cb_cell).
@@ -285,14 +242,8 @@ static inline cudaError_t cb_launch_colwarp(CBParams<float> &p, int na, int nb, 
 {
     dim3 grid, block;
     cb_colwarp_shape(p, na, nb, nvc, grid, block);
-    if (!FWD && tune_get(NEFCT_TUNE_CB_COMBINE)) {
-        if (cubic(p.g)) cb_colwarp_kernel<false, FWD, true><<<grid, block, 0, s>>>(p);
-        else cb_colwarp_kernel<true, FWD, true><<<grid, block, 0, s>>>(p);
-    } else if (cubic(p.g)) {
-        cb_colwarp_kernel<false, FWD><<<grid, block, 0, s>>>(p);
-    } else {
-        cb_colwarp_kernel<true, FWD><<<grid, block, 0, s>>>(p);
-    }
+    if (cubic(p.g)) cb_colwarp_kernel<false, FWD><<<grid, block, 0, s>>>(p);
+    else cb_colwarp_kernel<true, FWD><<<grid, block, 0, s>>>(p);
     return cudaGetLastError();
 }
 

@@ -83,7 +83,10 @@ def test_fdk_distance_weight_pinned_by_reference_kernel(cuda, oracle_lib, phi):
     assert inside.sum() > 0.3 * n ** 3
     w_ref = ref_w[inside] / ours_nw[inside]
     w_ours = fw[inside] / fnw[inside]
-    np.testing.assert_allclose(w_ours, w_ref, rtol=5e-6)
+    # float32: each side is a ratio of two sums of ~20 rounded footprint
+    # terms (atomic order differs between the host build and the GPU), so
+    # agreement is to a few 1e-6; a wrong weight formula is off by ~1e-1
+    np.testing.assert_allclose(w_ours, w_ref, rtol=2e-5)
 
 
 def test_weighted_backprojection_vs_oracle(cuda, oracle_lib):

@@ -514,36 +514,3 @@ def test_forward_transpose_capture_in_cuda_graph(cuda):
     assert torch.equal(sino, ref_s)
     assert_parity(back.cpu().numpy(), ref_b.cpu().numpy(), rel=1e-6, mabs=1e-5)
 
-
-@pytest.mark.parametrize("name", ["steep_cone", "odd_counts", "one_row", "thin_grid"])
-@pytest.mark.parametrize("fine_rows", [False, True], ids=["rows-wider-than-voxels", "rows-finer-than-voxels"])
-def test_transpose_run_combining(cuda, oracle_lib, name, fine_rows):
-    """NEFCT_TUNE_CB_COMBINE=1 sums the contributions of neighbouring rows
-    on the same voxel before one reduction: the same contributions as the
-    plain column-warp transpose (only the float summation order differs),
-    against the oracle's exact transpose -- with detector rows wider than a
-    voxel at the volume (no runs) and 8x finer (runs of ~4-8 lanes, up to
-    the whole warp in the steep cone), non-cubic voxels in odd_counts."""
-    from nefct_b200 import autotune
-    e = dict(_EDGE[name])
-    if fine_rows:
-        e["db"] = e["db"] / 8
-        e["nb"] = min(e["nb"] * 4, 256)
-    size = tuple(float(v) * (1.0, 1.3, 0.8)[i] if name == "odd_counts" else float(v)
-                 for i, v in enumerate(e["shape"]))
-    g = nb.ConeBeam(e["shape"], _EDGE_ANGLES, e["src_iso"], e["src_det"], e["na"], e["da"], e["nb"], e["db"],
-                    size=size)
-    y = np.random.default_rng(17).random(g.sino_shape, dtype=np.float32)
-    og = oracle_lib.grid(e["shape"], (0, 0, 0), size)
-    args = (_EDGE_ANGLES, e["src_iso"], e["src_det"], e["na"], e["da"], 0.5, e["nb"], e["db"], 0.5)
-    ref = oracle_lib.cb_backward(og, y, *args, flags=oracle_lib.CB_FWD)
-    saved = autotune.current()
-    outs = {}
-    try:
-        for cmb in (0, 1):
-            autotune.apply(saved["rows"], saved["order"], 3, cmb)
-            outs[cmb] = ops.cb_backward(torch.from_numpy(y).to(cuda), g).cpu().numpy()
-    finally:
-        autotune.apply(saved["rows"], saved["order"], saved["walk"], saved["combine"])
-    assert_parity(outs[1], ref, rel=1e-6, mabs=1e-5)
-    assert_parity(outs[1], outs[0], rel=1e-6, mabs=1e-5)

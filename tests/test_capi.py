@@ -147,3 +147,29 @@ def test_noalloc_refuses_grids_beyond_its_scratch(nefct_lib):
     st = nefct_lib.nefct_cb_forward_noalloc(C.byref(s), C.c_void_p(256), C.c_void_p(256), 0, None)
     assert st == _lib.ERR_INVALID
     assert b"at most 8388608 voxels" in nefct_lib.nefct_last_error()
+
+
+def test_dd_pair_rejects_bad_arguments(nefct_lib):
+    """The distance-driven pair validates geometry, flags, buffers and the
+    workspace before any CUDA call."""
+    from nefct_b200 import _lib, ops
+    g = ops.DDGeometry((8, 8, 8), np.linspace(0, 3, 4), 50.0, 100.0, 16, 1.0, 8, 1.0)
+    s = g.struct()
+    ws = C.c_void_p(256)
+    assert nefct_lib.nefct_dd_forward(C.byref(s), C.c_void_p(256), C.c_void_p(256), 0x1, ws, 1 << 20, None) == \
+        _lib.ERR_INVALID
+    assert b"unknown flag" in nefct_lib.nefct_last_error()
+    assert nefct_lib.nefct_dd_forward(C.byref(s), None, C.c_void_p(256), 0, ws, 1 << 20, None) == _lib.ERR_INVALID
+    st = nefct_lib.nefct_dd_backward(C.byref(s), C.c_void_p(256), C.c_void_p(256), 0, ws, 16, None)
+    assert st == _lib.ERR_WORKSPACE and b"workspace" in nefct_lib.nefct_last_error()
+    bad = ops.DDGeometry((0, 8, 8), np.linspace(0, 3, 4), 50.0, 100.0, 16, 1.0, 8, 1.0).struct()
+    assert nefct_lib.nefct_dd_forward_f64(C.byref(bad), C.c_void_p(256), C.c_void_p(256), 0, None) == \
+        _lib.ERR_INVALID
+
+
+def test_probes_reject_bad_arguments(nefct_lib):
+    from nefct_b200 import _lib
+    assert nefct_lib.nefct_probe_l2_read(C.c_void_p(256), 6, 1, 8, C.c_void_p(256), None) == _lib.ERR_INVALID
+    assert nefct_lib.nefct_probe_l2_read(C.c_void_p(260), 8, 1, 8, C.c_void_p(256), None) == _lib.ERR_INVALID
+    assert nefct_lib.nefct_probe_l2_red(C.c_void_p(256), 8, 0, 8, None) == _lib.ERR_INVALID
+    assert nefct_lib.nefct_probe_l2_red(None, 8, 1, 8, None) == _lib.ERR_INVALID

@@ -20,8 +20,10 @@
 // table is exhausted.  Tickets never wait on anything, so the kernel cannot
 // hang; load balance across uneven problems comes from the dynamic dequeue
 // and the longest-first order.  Forward and transpose are each one
-// persistent launch plus per-problem transposes/folds; all work is
-// stream-ordered and capturable in a CUDA graph after nefct_cb_batch_bind.
+// persistent launch plus the volume copies / folds (with column warps: one
+// launch over all problems' tiles, and one memset of all accumulators, which
+// are contiguous in the workspace); all work is stream-ordered and
+// capturable in a CUDA graph after nefct_cb_batch_bind.
 //
 // Device workspace (caller-owned), 256-byte aligned sections:
 //   counters[4] | view tables | per-problem volume copy
@@ -66,6 +68,7 @@ static constexpr int kMaxBatch = 96;
 struct BatchArgs {
     BatchDesc d[kMaxBatch];
     long long t0[kMaxBatch + 1];
+    long long c0[kMaxBatch + 1];         // offsets of the problems' 32 x 32 copy tiles (column warps)
     int n;
     long long begin, end;
     unsigned long long *counter;
@@ -79,6 +82,7 @@ struct BatchPlan {
     std::vector<int> order;                // plan order -> caller index
     std::vector<BatchDesc> desc;           // plan order (device pointers filled at bind)
     std::vector<long long> t0;             // tile offsets, n + 1
+    std::vector<long long> c0;             // copy-tile offsets, n + 1 (z-fastest copies and folds)
     std::vector<float> views;              // cs | sn | off per problem, plan order
     std::vector<size_t> view_off, vol_off; // float offsets in the workspace sections
     uint32_t flags = 0;
@@ -103,6 +107,49 @@ __device__ __forceinline__ int find_problem(const long long *t0, int n, long lon
         else hi = mid - 1;
     }
     return lo;
+}
+
+// The z-fastest copies (FOLD false: vol[z][y][x] -> volT[y][x][z]) or folds
+// (FOLD true: volT -> back[z][y][x]) of every problem in one launch: the
+// 32 x 32 (x, z) tiles of all problems' y planes, tile t of problem p at
+// c0[p] + ((y * tiles_z) + tz) * tiles_x + tx, grid-strided.
+template <bool FOLD>
+__global__ void __launch_bounds__(256) batch_zcopy_kernel(const __grid_constant__ BatchArgs a, long long total)
+{
+    __shared__ float tile[32][33];
+    for (long long t = blockIdx.x; t < total; t += gridDim.x) {     // uniform across the CTA
+        const int p = find_problem(a.c0, a.n, t);
+        const BatchDesc &P = a.d[p];
+        const int nx = P.g.nx, ny = P.g.ny, nz = P.g.nz;
+        const int tiles_x = (nx + 31) / 32, tiles_z = (nz + 31) / 32;
+        const long long local = t - a.c0[p];
+        const int x0 = (int)(local % tiles_x) * 32;
+        const long long rest = local / tiles_x;
+        const int z0 = (int)(rest % tiles_z) * 32;
+        const int y = (int)(rest / tiles_z);
+        if (!FOLD) {
+            for (int j = threadIdx.y; j < 32; j += 8) {
+                const int x = x0 + threadIdx.x, z = z0 + j;
+                if (x < nx && z < nz) tile[j][threadIdx.x] = P.vol[((size_t)z * ny + y) * nx + x];
+            }
+            __syncthreads();
+            for (int j = threadIdx.y; j < 32; j += 8) {
+                const int x = x0 + j, z = z0 + threadIdx.x;
+                if (x < nx && z < nz) P.volT[((size_t)y * nx + x) * nz + z] = tile[threadIdx.x][j];
+            }
+        } else {
+            for (int j = threadIdx.y; j < 32; j += 8) {
+                const int x = x0 + j, z = z0 + threadIdx.x;
+                if (x < nx && z < nz) tile[j][threadIdx.x] = P.volT[((size_t)y * nx + x) * nz + z];
+            }
+            __syncthreads();
+            for (int j = threadIdx.y; j < 32; j += 8) {
+                const int x = x0 + threadIdx.x, z = z0 + j;
+                if (x < nx && z < nz) P.back[((size_t)z * ny + y) * nx + x] = tile[threadIdx.x][j];
+            }
+        }
+        __syncthreads();                  // the tile is read before the next iteration rewrites it
+    }
 }
 
 // One persistent launch serves tiles [begin, end) of problems that share
@@ -214,19 +261,28 @@ static nefct_status batch_launch(BatchPlan *b, bool fwd, cudaStream_t s)
     const int n = (int)b->desc.size();
     unsigned long long *counter = (unsigned long long *)b->ws + (fwd ? 0 : 2);
     NEFCT_CHECK_CUDA(cudaMemsetAsync(counter, 0, 2 * sizeof(unsigned long long), s));
-    for (int i = 0; i < n; ++i) {
+    BatchArgs &ca = *b->args;
+    const long long copy_tiles = b->c0.back();
+    const unsigned copy_blocks = (unsigned)std::min<long long>(copy_tiles, 148ll * 8);
+    if (b->colwarp) {
+        // one launch for all problems' z-fastest copies (forward) or one memset
+        // of every accumulator (transpose; they are contiguous in the workspace)
+        if (fwd) {
+            batch_zcopy_kernel<false><<<copy_blocks, dim3(32, 8), 0, s>>>(ca, copy_tiles);
+            NEFCT_CHECK_LAUNCH("batch_zcopy_kernel");
+        } else {
+            NEFCT_CHECK_CUDA(cudaMemsetAsync(b->ws + b->off_vols, 0, b->bytes - b->off_vols, s));
+        }
+    }
+    for (int i = 0; i < n && !b->colwarp; ++i) {
         const BatchDesc &D = b->desc[i];
-        const nefct_cb_geom &g = b->probs[b->order[i]].geom;
         const size_t nvox = (size_t)D.g.nx * D.g.ny * D.g.nz;
         dim3 tg((D.g.nx + 31) / 32, (D.g.ny + 31) / 32, D.g.nz);
-        if (fwd && b->colwarp) {
-            nefct_status st = zmajor_copy(D.vol, D.volT, g.grid, s);
-            if (st) return st;
-        } else if (fwd) {
+        if (fwd) {
             transpose_xy_kernel<float><<<tg, dim3(32, 8), 0, s>>>(D.vol, D.volT, D.g.nx, D.g.ny);
             NEFCT_CHECK_LAUNCH("transpose_xy_kernel (batch)");
         } else {
-            if (!b->colwarp) NEFCT_CHECK_CUDA(cudaMemsetAsync(D.back, 0, nvox * sizeof(float), s));
+            NEFCT_CHECK_CUDA(cudaMemsetAsync(D.back, 0, nvox * sizeof(float), s));
             NEFCT_CHECK_CUDA(cudaMemsetAsync(D.volT, 0, nvox * sizeof(float), s));
         }
     }
@@ -255,14 +311,12 @@ static nefct_status batch_launch(BatchPlan *b, bool fwd, cudaStream_t s)
         }
         NEFCT_CHECK_LAUNCH("batch_kernel (other voxels)");
     }
-    if (!fwd) {
+    if (!fwd && b->colwarp) {
+        batch_zcopy_kernel<true><<<copy_blocks, dim3(32, 8), 0, s>>>(ca, copy_tiles);
+        NEFCT_CHECK_LAUNCH("batch_zcopy_kernel (fold)");
+    } else if (!fwd) {
         for (int i = 0; i < n; ++i) {
             const BatchDesc &D = b->desc[i];
-            if (b->colwarp) {
-                nefct_status st = zfold(D.volT, D.back, b->probs[b->order[i]].geom.grid, s);
-                if (st) return st;
-                continue;
-            }
             dim3 tg((D.g.nx + 31) / 32, (D.g.ny + 31) / 32, D.g.nz);
             fold_add_kernel<float><<<tg, dim3(32, 8), 0, s>>>(D.volT, D.back, D.g.nx, D.g.ny);
             NEFCT_CHECK_LAUNCH("fold_add_kernel (batch)");
@@ -332,6 +386,7 @@ nefct_status nefct_cb_batch_plan(const nefct_cb_problem *problems, int32_t n, ui
     });
     b->desc.resize(n);
     b->t0.assign(n + 1, 0);
+    b->c0.assign(n + 1, 0);
     size_t views = 0, vols = 0;
     b->view_off.resize(n);
     b->vol_off.resize(n);
@@ -346,6 +401,7 @@ nefct_status nefct_cb_batch_plan(const nefct_cb_problem *problems, int32_t n, ui
         D.cubic = D.g.dy == 1.f && D.g.dz == 1.f;
         D.flags = flags;
         b->t0[k + 1] = b->t0[k] + (long long)D.tiles_a * D.tiles_b * g.nv;
+        b->c0[k + 1] = b->c0[k] + (long long)((g.grid.nx + 31) / 32) * ((g.grid.nz + 31) / 32) * g.grid.ny;
         if (D.cubic) b->split = b->t0[k + 1];
         b->view_off[k] = views;
         views += 3 * (size_t)g.nv;
@@ -392,6 +448,7 @@ nefct_status nefct_cb_batch_bind(nefct_cb_batch *b, void *workspace, size_t byte
     if (!b->args) b->args = new BatchArgs();
     std::copy(b->desc.begin(), b->desc.end(), b->args->d);
     std::copy(b->t0.begin(), b->t0.end(), b->args->t0);
+    std::copy(b->c0.begin(), b->c0.end(), b->args->c0);
     b->args->n = n;
     NEFCT_CHECK_CUDA(cudaMemcpyAsync(ws + b->off_views, b->views.data(), b->views.size() * sizeof(float),
                                      cudaMemcpyHostToDevice, s));

@@ -229,7 +229,8 @@ void nefct_cb_batch_destroy(nefct_cb_batch *plan);
  * entry points projection / backprojection (siddon_gpu.cu.cc:700-747).
  * nefct_lor_forward writes every out[i] (0 for rays the reference skips
  * without writing, Q4); nefct_lor_backward overwrites vol (the reference op
- * accumulates into an unzeroed buffer, Q6). */
+ * accumulates into an unzeroed buffer, Q6).  n = 0 is valid: the forward
+ * writes nothing (its buffers may be NULL), the backward zeroes vol. */
 nefct_status nefct_lor_forward(const nefct_grid *grid, const float *lors, int64_t n, const float *vol,
                                float *out, uint32_t flags, void *stream);
 nefct_status nefct_lor_backward(const nefct_grid *grid, const float *lors, int64_t n, const float *vals,

@@ -578,6 +578,7 @@ static nefct_status lor_impl(const nefct_grid *grid, const T *lors, int64_t n, c
         return fail(NEFCT_ERR_UNSUPPORTED, "the LOR projector takes the walk flags of cpp/siddon only");
     if ((!lors || !src || !dst) && n > 0) return fail(NEFCT_ERR_INVALID, "NULL buffer");
     if (flags & ~kWalkFlags) return fail(NEFCT_ERR_INVALID, "unknown flag bits 0x%x", flags & ~kWalkFlags);
+    if (forward && n == 0) return NEFCT_OK;          // no lines: nothing to write
     if (!dst) return fail(NEFCT_ERR_INVALID, "NULL output");
     LorParams<T> p;
     p.g = make_grid_dev<T>(*grid);

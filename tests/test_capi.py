@@ -173,3 +173,25 @@ def test_probes_reject_bad_arguments(nefct_lib):
     assert nefct_lib.nefct_probe_l2_read(C.c_void_p(260), 8, 1, 8, C.c_void_p(256), None) == _lib.ERR_INVALID
     assert nefct_lib.nefct_probe_l2_red(C.c_void_p(256), 8, 0, 8, None) == _lib.ERR_INVALID
     assert nefct_lib.nefct_probe_l2_red(None, 8, 1, 8, None) == _lib.ERR_INVALID
+
+
+@pytest.mark.parametrize("kw,needle", [
+    (dict(shape=((1 << 20) + 1, 1, 1)), b"<= 2^20"),
+    (dict(shape=(2048, 2048, 1024)), b"2^31"),
+    (dict(nb=65536), b"65535"),
+])
+def test_size_limits_are_rejected(nefct_lib, kw, needle):
+    """Grid dimensions above 2^20, grids of 2^31 voxels or more and more than
+    65535 detector rows are refused with a status before any CUDA call."""
+    g = _geom(**kw).struct()
+    st = nefct_lib.nefct_cb_forward(C.byref(g), C.c_void_p(256), C.c_void_p(256), 0, C.c_void_p(256), 1 << 40,
+                                    None)
+    assert st == 1
+    assert needle in nefct_lib.nefct_last_error()
+
+
+def test_lor_negative_count_is_rejected(nefct_lib):
+    from nefct_b200 import _lib
+    grid = _lib.Grid(8, 8, 8, 0, 0, 0, 8, 8, 8)
+    assert nefct_lib.nefct_lor_forward(C.byref(grid), C.c_void_p(256), -1, C.c_void_p(256), C.c_void_p(256), 0,
+                                       None) == _lib.ERR_INVALID

@@ -120,3 +120,25 @@ def test_lor_op_mirrors_order_long_lists(cuda):
     b = nb.cc.siddon.backprojection(image, lors, vals, shape, center, size).double()
     b0 = ops.lor_backward(lors, vals, shape, center, size, _lib.LOR_REF_BACKPROJECT).view(image.shape).double()
     assert float((b - b0).norm() / b0.norm()) < 1e-6
+
+
+def test_empty_and_degenerate_inputs(cuda):
+    """An empty LOR list gives an empty forward and a zero backprojection; a
+    zero sinogram transposes to an exactly zero volume; a one-voxel grid seen
+    by a 1 x 1 detector in one view projects and transposes consistently."""
+    from nefct_b200 import ops
+    vol = torch.rand((8, 8, 8), device=cuda)
+    lors = torch.empty((6, 0), device=cuda)
+    assert ops.lor_forward(lors, vol, (8, 8, 8)).numel() == 0
+    bp = ops.lor_backward(lors, torch.empty(0, device=cuda), (8, 8, 8))
+    assert bp.shape == (8, 8, 8) and float(bp.abs().max()) == 0.0
+    g = nb.ConeBeam((8, 8, 8), np.linspace(0, 2 * np.pi, 7, endpoint=False), 40.0, 80.0, 12, 1.0, 10, 1.0)
+    back = ops.cb_backward(torch.zeros(g.sino_shape, device=cuda), g)
+    assert float(back.abs().max()) == 0.0
+    g1 = nb.ConeBeam((1, 1, 1), [0.3], 40.0, 80.0, 1, 2.0, 1, 2.0, size=(1.0, 1.0, 1.0))
+    x = torch.full((1, 1, 1), 3.0, device=cuda)
+    y = torch.full((1, 1, 1), 2.0, device=cuda)
+    ax = ops.cb_forward(x, g1)
+    aty = ops.cb_backward(y, g1)
+    assert float(ax) > 0
+    assert abs(float((ax * y).sum()) - float((x * aty).sum())) <= 1e-6 * float((ax * y).sum())

@@ -23,5 +23,6 @@ from .functions import (FDK, SART, BackProject3D, BackProject3DT, ConjGrad, Proj
                         WarpDeformer, cone_beam)
 from . import cc
 from . import recon
+from .io import json_dump, json_dumps, json_load, json_loads, load, save
 
 __version__ = "0.1.0"

@@ -3,7 +3,8 @@
 Mirrors nefct/base/base.py:29-177 (NefBaseClass / nef_class): every
 annotated field becomes an optional attrs attribute (default None unless the
 class gives one), instances are frozen, and ``update`` / ``asdict`` /
-``keys`` / ``values`` / ``items`` behave as in the reference.
+``keys`` / ``values`` / ``items`` / ``from_dict`` / ``astype`` behave as in
+the reference.
 """
 from __future__ import annotations
 
@@ -28,6 +29,43 @@ class NefBaseClass:
 
     def asdict(self, recurse: bool = False) -> dict:
         return attr.asdict(self, recurse=recurse)
+
+    @classmethod
+    def from_dict(cls, dct: dict):
+        """Instance from a dict of field values (nefct/base/base.py:98-118):
+        missing keys stay None, a nested dict becomes the annotated
+        nef_class of its field, numpy booleans become bool."""
+        import numpy as np
+        if dct is None:
+            return cls()
+        hints = _field_types(cls)
+        kwargs = {}
+        for key in cls.keys():
+            if key not in dct:
+                continue
+            val = dct[key]
+            type_ = hints.get(key)
+            if isinstance(val, dict) and isinstance(type_, type) and issubclass(type_, NefBaseClass):
+                val = type_.from_dict(val)
+            elif isinstance(val, np.bool_):
+                val = bool(val)
+            kwargs[key] = val
+        return cls(**kwargs)
+
+    def astype(self, cls: type):
+        """The same fields as another nef_class (base.py:120-121)."""
+        return cls.from_dict(self.asdict(recurse=True))
+
+
+def _field_types(cls) -> dict:
+    """Field annotations resolved to classes (modules here use postponed
+    annotations, so they are strings until resolved)."""
+    import sys
+    import typing
+    try:
+        return typing.get_type_hints(cls, vars(sys.modules[cls.__module__]))
+    except Exception:
+        return {}
 
 
 def nef_class(cls):

@@ -40,8 +40,22 @@ class _ArithmeticMixin:
     def __neg__(self): return self.update(data=-self.data)
 
 
+class _SaveLoadMixin:
+    """obj.save(path) / Cls.load(path) (nefct/io/local_io_mixin.py:14-40),
+    through nefct_b200.io."""
+
+    def save(self, path: str) -> str:
+        from .io import save
+        return save(self, path)
+
+    @classmethod
+    def load(cls, path: str, partial=None):
+        from .io import load
+        return load(cls, path, partial)
+
+
 @nef_class
-class Image(_ArithmeticMixin):
+class Image(_ArithmeticMixin, _SaveLoadMixin):
     data: object
     center: list
     size: list
@@ -92,7 +106,7 @@ def all_zero_image(*args, **kwargs):
 
 
 @nef_class
-class ProjectionSequence3D(_ArithmeticMixin):
+class ProjectionSequence3D(_ArithmeticMixin, _SaveLoadMixin):
     data: object
     scanner: ScannerConfig3D
     angles: list

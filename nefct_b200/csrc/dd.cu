@@ -107,6 +107,7 @@ template <typename T, bool FWD>
 __global__ void __launch_bounds__(256) dd_kernel(const __grid_constant__ DDParams<T> p)
 {
     using F = FP<T>;
+    constexpr bool kF32 = sizeof(T) == sizeof(float);
     const int lane = threadIdx.x;
     const int ia = blockIdx.x * blockDim.y + threadIdx.y;
     const int ib = blockIdx.y * 32 + lane;
@@ -184,20 +185,24 @@ __global__ void __launch_bounds__(256) dd_kernel(const __grid_constant__ DDParam
                 const T iden = dd_rcp(den);
                 fw = F::mul(F::mul(sad2, iden), iden);
             }
+            // the float path walks the z-fastest copy: unit z stride
             const size_t col = (size_t)iy * p.sy + (size_t)ix * p.sx;
+            const size_t zs = kF32 ? 1 : (size_t)p.sz;
             if (FWD) {
                 // wv * (len / |u21|) * fw per voxel of the column, times wz
                 const T cw = F::mul(F::mul(wv, len_au), fw);
+                const T *c = p.src + col;
                 for (int iz = za; iz <= zb; ++iz) {
                     const T wz = F::mul(F::sub(dd_min((T)iz + (T)1, zi2), dd_max((T)iz, zi1)), izspan);
-                    acc = F::add(acc, F::mul(__ldg(p.src + col + (size_t)iz * p.sz), F::mul(cw, wz)));
+                    acc = F::add(acc, F::mul(__ldg(c + (size_t)iz * zs), F::mul(cw, wz)));
                 }
             } else {
                 // value * wv * (len / |u21|) * fw per voxel of the column, times wz
                 const T cw = F::mul(F::mul(F::mul(value, wv), len_au), fw);
+                T *c = p.dst + col;
                 for (int iz = za; iz <= zb; ++iz) {
                     const T wz = F::mul(F::sub(dd_min((T)iz + (T)1, zi2), dd_max((T)iz, zi1)), izspan);
-                    atomicAdd(p.dst + col + (size_t)iz * p.sz, F::mul(cw, wz));
+                    atomicAdd(c + (size_t)iz * zs, F::mul(cw, wz));
                 }
             }
         }

@@ -685,7 +685,8 @@ def run_batched(args):
                     f"detector U[128,1024]^2 x{args.scale}, seed 4")
     gen = torch.Generator(device=dev).manual_seed(4)
     vols = [torch.rand(g.vol_shape, device=dev, generator=gen) for g in geoms]
-    bp = BatchProjector(geoms, vols)            # grads = the forward outputs (loss = |Ax|^2 / 2)
+    # grads = the forward outputs (loss = |Ax|^2 / 2); tile shape autotuned for the small regime
+    bp = BatchProjector(geoms, vols, tune_rows=args.regime == "small")
     inter = sum(ops.cb_count_intersections(g, 0, dev) for g in geoms)
 
     def timed(fn, reps):
@@ -711,10 +712,15 @@ def run_batched(args):
     best = min(strategies, key=strategies.get)
     bp.set_strategy(best)
 
-    # one autograd iteration through the batched Function
+    # one autograd iteration through the batched Function (a plan of the same tile shape)
+    from nefct_b200 import autotune
     xs = [v.clone().requires_grad_() for v in vols]
+    saved = autotune.current()
+    if bp.tuned_rows:
+        autotune.apply(bp.tuned_rows["rows"], saved["order"])
     grads_bp = BatchProjector(geoms, [v.detach().clone() for v in vols],
                               grads=[torch.empty(g.sino_shape, device=dev) for g in geoms], strategy=best)
+    autotune.apply(saved["rows"], saved["order"])
 
     def autograd_batched():
         for x in xs:
@@ -763,6 +769,7 @@ def run_batched(args):
             "config": {"workload": workload, "voxels": int(sum(np.prod(g.shape) for g in geoms)),
                        "rays": int(sum(g.nv * g.na * g.nb for g in geoms)), "tiles": bp.tiles},
             "extras": {"strategy": best, "graph_replay_ms_by_strategy": strategies,
+                       "tile_shape_tuning": bp.tuned_rows,
                        "intersections_per_iteration": 2 * inter,
                        "batched_graph_replay_ms": 1e3 * t_batch,
                        "batched_autograd_ms": 1e3 * t_autograd,

@@ -63,7 +63,7 @@ def batch_project(bp: "BatchProjector", vols: list) -> tuple:
 
 class BatchProjector:
     def __init__(self, geoms: list[ops.ConeBeam], vols: list[torch.Tensor], sinos=None, grads=None, backs=None,
-                 flags: int = 0, strategy: str = "auto"):
+                 flags: int = 0, strategy: str = "auto", tune_rows: bool = False):
         if len(geoms) != len(vols) or not geoms:
             raise ValueError("need one volume per geometry")
         dev = vols[0].device
@@ -77,6 +77,10 @@ class BatchProjector:
         self.backs = backs or [torch.empty(g.vol_shape, device=dev) for g in geoms]
         self.flags = flags
         self.device = dev
+        self.tuned_rows = None
+        if tune_rows:
+            self.tuned_rows = self._tune_rows(strategy)
+            strategy = self.tuned_rows["strategy"]
         n = len(geoms)
         probs = (_lib.CBProblem * n)()
         self._structs = []
@@ -89,7 +93,12 @@ class BatchProjector:
         lib = _lib.load()
         plan = C.c_void_p()
         nbytes = C.c_size_t()
-        _lib.check(lib.nefct_cb_batch_plan(probs, n, flags, C.byref(plan), C.byref(nbytes)))
+        try:
+            _lib.check(lib.nefct_cb_batch_plan(probs, n, flags, C.byref(plan), C.byref(nbytes)))
+        finally:
+            if self.tuned_rows is not None:          # the plan has fixed its rows: restore the caller's
+                from . import autotune
+                autotune.apply(self.tuned_rows["saved_rows"], self.tuned_rows["saved_order"])
         self._plan = plan
         self.workspace = torch.empty(nbytes.value, dtype=torch.uint8, device=dev)
         with torch.cuda.device(dev):
@@ -100,6 +109,39 @@ class BatchProjector:
         if strategy == "auto":
             strategy = self._pick()
         self.set_strategy(strategy)
+
+    def _tune_rows(self, strategy: str) -> dict:
+        """Autotunes the plan's tile shape: times one step of a plan with 2,
+        4 and 8 rows (columns, for column warps) per CTA under each strategy
+        and applies the fastest rows setting (NEFCT_TUNE_CB_ROWS) for the
+        plan to fix; the caller's setting is restored once it has."""
+        from . import autotune
+        saved = autotune.current()
+        times = {}
+        try:
+            for rows in (2, 4, 8):
+                autotune.apply(rows, saved["order"])
+                trial = BatchProjector(self.geoms, self.vols, sinos=self.sinos, grads=self.grads, backs=self.backs,
+                                       flags=self.flags, strategy=strategy)
+                for name, ms in (trial.timings or {trial.strategy: None}).items():
+                    if ms is None:
+                        trial.step()
+                        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                        e0.record()
+                        trial.step()
+                        e1.record()
+                        e1.synchronize()
+                        ms = e0.elapsed_time(e1)
+                    times[f"{rows}/{name}"] = ms
+                del trial
+            best = min(times, key=times.get)
+            rows, strat = best.split("/")
+            autotune.apply(int(rows), saved["order"])
+            return {"rows": int(rows), "strategy": strat, "ms": times, "saved_rows": saved["rows"],
+                    "saved_order": saved["order"]}
+        except Exception:
+            autotune.apply(saved["rows"], saved["order"])
+            raise
 
     def set_strategy(self, strategy: str) -> None:
         code = {"persistent": _lib.BATCH_PERSISTENT, "per-problem": _lib.BATCH_PER_PROBLEM}[strategy]

@@ -141,3 +141,21 @@ def test_batch_autograd_function(cuda):
         xr = x.detach().clone().requires_grad_()
         (((nb.project(xr, g) - t) ** 2).sum() / 2).backward()
         assert_parity(x.grad.cpu().numpy(), xr.grad.cpu().numpy())
+
+
+def test_batch_tile_shape_autotuning(cuda):
+    """tune_rows=True times plans with 2, 4 and 8 rows (columns) per CTA under
+    both strategies, keeps the fastest, restores the process-wide setting,
+    and the tuned plan gives the single-problem results."""
+    from nefct_b200 import autotune
+    geoms, vols, grads = _problems(cuda)
+    before = autotune.current()
+    bp = BatchProjector(geoms, vols, grads=grads, tune_rows=True)
+    assert autotune.current() == before
+    assert bp.tuned_rows["rows"] in (2, 4, 8) and bp.strategy == bp.tuned_rows["strategy"]
+    assert len(bp.tuned_rows["ms"]) == 6
+    bp.step()
+    torch.cuda.synchronize()
+    for g, v, gr, s, b in zip(geoms, vols, grads, bp.sinos, bp.backs):
+        assert torch.equal(s, ops.cb_forward(v, g))
+        assert_parity(b.cpu().numpy(), ops.cb_backward(gr, g).cpu().numpy())

@@ -277,6 +277,14 @@ nefct_status nefct_fdk_filter(const nefct_cb_geom *g, const float *sino, float *
 #define NEFCT_FDK_NO_WEIGHT 0x100u
 nefct_status nefct_fdk_backproject(const nefct_cb_geom *g, const float *filtered, float *vol, uint32_t flags,
                                    void *stream);
+/* The same backprojection with a caller workspace (nefct_fdk_workspace_bytes,
+ * 16-byte aligned; NULL gives nefct_fdk_backproject): each chunk of views
+ * is first repacked into tap quads (the four bilinear taps of every detector
+ * cell side by side) so a voxel reads its taps with one 16-byte load.  Same
+ * arithmetic, bit-identical result.  No counterpart in the reference. */
+size_t nefct_fdk_workspace_bytes(const nefct_cb_geom *g);
+nefct_status nefct_fdk_backproject_ws(const nefct_cb_geom *g, const float *filtered, float *vol, uint32_t flags,
+                                      void *ws, size_t ws_bytes, void *stream);
 
 /* Trilinear warp of cpp/deform (DeformKernel deform.cu.cc:13-46, op Deform
  * deform.cc:12-22): out[i] = trilinear(img, i + m[i]), displacements in

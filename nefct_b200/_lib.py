@@ -105,6 +105,8 @@ _PROTOS = {
     "nefct_lor_backward_ordered": (_i32, [C.POINTER(Grid), _vp, C.c_int64, _vp, _vp, _vp, _u32, _vp]),
     "nefct_fdk_filter": (_i32, [C.POINTER(CBGeom), _vp, _vp, _i32, _i32, _vp]),
     "nefct_fdk_backproject": (_i32, [C.POINTER(CBGeom), _vp, _vp, _u32, _vp]),
+    "nefct_fdk_workspace_bytes": (C.c_size_t, [C.POINTER(CBGeom)]),
+    "nefct_fdk_backproject_ws": (_i32, [C.POINTER(CBGeom), _vp, _vp, _u32, _vp, C.c_size_t, _vp]),
     "nefct_warp_forward": (_i32, [_vp, _vp, _vp, _vp, _i32, _i32, _i32, _vp, _vp]),
     "nefct_warp_adjoint": (_i32, [_vp, _vp, _vp, _vp, _i32, _i32, _i32, _vp, _vp]),
     "nefct_warp_grad_dvf": (_i32, [_vp, _vp, _vp, _vp, _vp, _i32, _i32, _i32, _vp, _vp, _vp, _vp]),

@@ -294,8 +294,11 @@ def fdk_backproject(filtered: torch.Tensor, geom: ConeBeam, weight: bool = True)
     out = torch.empty(geom.vol_shape, dtype=torch.float32, device=filtered.device)
     with torch.cuda.device(filtered.device):
         g = geom.struct()
-        _lib.call("nefct_fdk_backproject", C.byref(g), filtered.data_ptr(), out.data_ptr(),
-                  0 if weight else _lib.FDK_NO_WEIGHT, _stream(filtered))
+        # tap-quad workspace (one chunk of views) from the caching allocator
+        wn = _lib.load().nefct_fdk_workspace_bytes(C.byref(g))
+        ws = torch.empty(wn, dtype=torch.uint8, device=filtered.device)
+        _lib.call("nefct_fdk_backproject_ws", C.byref(g), filtered.data_ptr(), out.data_ptr(),
+                  0 if weight else _lib.FDK_NO_WEIGHT, ws.data_ptr(), wn, _stream(filtered))
     return out
 
 

@@ -195,3 +195,16 @@ def test_lor_negative_count_is_rejected(nefct_lib):
     grid = _lib.Grid(8, 8, 8, 0, 0, 0, 8, 8, 8)
     assert nefct_lib.nefct_lor_forward(C.byref(grid), C.c_void_p(256), -1, C.c_void_p(256), C.c_void_p(256), 0,
                                        None) == _lib.ERR_INVALID
+
+
+def test_fdk_quad_workspace_is_checked(nefct_lib):
+    from nefct_b200 import _lib
+    g = _geom().struct()
+    need = nefct_lib.nefct_fdk_workspace_bytes(C.byref(g))
+    assert need == 8 * 32 * 24 * 16          # all 8 views fit one chunk of tap quads
+    st = nefct_lib.nefct_fdk_backproject_ws(C.byref(g), C.c_void_p(256), C.c_void_p(256), 0, C.c_void_p(256),
+                                            need - 16, None)
+    assert st == _lib.ERR_WORKSPACE
+    st = nefct_lib.nefct_fdk_backproject_ws(C.byref(g), C.c_void_p(256), C.c_void_p(256), 0, C.c_void_p(264),
+                                            need, None)
+    assert st == _lib.ERR_INVALID and b"aligned" in nefct_lib.nefct_last_error()

@@ -143,3 +143,31 @@ def test_short_scan_parker_close_to_full_scan(cuda):
     for sign in (1, -1):
         assert errs[(sign, 1)] < 0.1, errs
         assert errs[(sign, -1)] > 1.5 * errs[(sign, 1)], errs
+
+
+@pytest.mark.parametrize("weight", [True, False])
+@pytest.mark.parametrize("cyl", [False, True], ids=["flat", "cyl"])
+def test_tap_quad_backprojection_is_bitwise_equal(cuda, weight, cyl):
+    """nefct_fdk_backproject_ws (taps read as quads from a repacked chunk)
+    gives the bits of nefct_fdk_backproject (four loads per tap set), over
+    several view chunks, with taps at the detector's last row and column."""
+    import ctypes as C
+    from nefct_b200 import _lib
+    lib = _lib.load()
+    nv = 70
+    g = nb.ConeBeam((40, 36, 30), np.linspace(0, 2 * np.pi, nv, endpoint=False), 90.0, 180.0, 61,
+                    0.02 if cyl else 1.3, 47, 1.2, size=(40.0, 36.0, 30.0), det_kind="cyl" if cyl else "flat")
+    sino = torch.rand(g.sino_shape, device=cuda, generator=torch.Generator(device=cuda).manual_seed(2))
+    s = g.struct()
+    flags = 0 if weight else _lib.FDK_NO_WEIGHT
+    stream = torch.cuda.current_stream(cuda).cuda_stream
+    plain = torch.empty(g.vol_shape, device=cuda)
+    _lib.check(lib.nefct_fdk_backproject(C.byref(s), sino.data_ptr(), plain.data_ptr(), flags, stream))
+    wn = lib.nefct_fdk_workspace_bytes(C.byref(s))
+    ws = torch.empty(wn, dtype=torch.uint8, device=cuda)
+    quad = torch.full(g.vol_shape, float("nan"), device=cuda)
+    _lib.check(lib.nefct_fdk_backproject_ws(C.byref(s), sino.data_ptr(), quad.data_ptr(), flags, ws.data_ptr(), wn,
+                                            stream))
+    torch.cuda.synchronize()
+    assert torch.equal(quad, plain)
+    assert float(plain.abs().max()) > 0

@@ -14,6 +14,10 @@ Two layers:
   host C++ from the reference sources (``ref_shim.cc``, ``Makefile``).  Used to
   pin the restatement and as the "reference" CPU baseline.  Present only when
   it was built (it needs the reference checkout at build time).
+* ``_ref/libnefct_ref_tex.so`` -- the reference's texture-based DVF inversion
+  (``deform_tex.cu.cc``) compiled by nvcc for the GPU (``ref_tex_shim.cu``):
+  hardware texture filtering has no host form, so this one checker runs on
+  the GPU, on device buffers.
 
 The FDK filter restatement of the MATLAB code lives in ``oracle.fdk``.
 """
@@ -28,6 +32,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(HERE, "liboracle.so")
 _REF = os.path.join(HERE, "_ref", "libnefct_ref.so")
+_REF_TEX = os.path.join(HERE, "_ref", "libnefct_ref_tex.so")
 
 TIE_GE, SKIP_SHORT, INV_L2, Q5_TRIPLE_L = 1, 2, 4, 8
 CB_FWD = TIE_GE | INV_L2
@@ -67,6 +72,39 @@ def lib() -> C.CDLL:
 
 def have_ref() -> bool:
     return os.path.exists(_REF)
+
+
+def have_ref_tex() -> bool:
+    return os.path.exists(_REF_TEX)
+
+
+_ref_tex = None
+
+
+def ref_tex_invert(mx, my, mz):
+    """The reference's DeformInvertKernel (deform_tex.cu.cc:78-99, 30
+    Gauss-Seidel passes over linear-filtered, clamp-addressed textures) run
+    through its host function invert() (:102-168) on the GPU.  mx, my, mz:
+    contiguous float32 CUDA tensors [nz][ny][nx]; returns the inverse field's
+    three components as new CUDA tensors.  Synchronises the device."""
+    import torch
+    global _ref_tex
+    if _ref_tex is None:
+        if not os.path.exists(_REF_TEX):
+            raise FileNotFoundError("oracle/_ref/libnefct_ref_tex.so was not built")
+        _ref_tex = C.CDLL(_REF_TEX)
+        _ref_tex.ref_tex_invert.restype = C.c_int
+        _ref_tex.ref_tex_invert.argtypes = [C.c_void_p] * 3 + [C.c_int] * 3 + [C.c_void_p] * 3
+    ms = [m.contiguous() for m in (mx, my, mz)]
+    for m in ms:
+        assert m.is_cuda and m.dtype == torch.float32 and m.dim() == 3
+    nz, ny, nx = ms[0].shape
+    out = [torch.empty_like(ms[0]) for _ in range(3)]
+    torch.cuda.synchronize()
+    err = _ref_tex.ref_tex_invert(*[m.data_ptr() for m in ms], nx, ny, nz, *[o.data_ptr() for o in out])
+    if err:
+        raise RuntimeError(f"reference texture inversion failed: CUDA error {err}")
+    return out
 
 
 def ref_threads() -> int:

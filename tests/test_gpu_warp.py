@@ -91,3 +91,38 @@ def test_warp_invert_vs_oracle(cuda, oracle_lib):
     ref = oracle_lib.warp_invert(*m, iters=30)
     for o, r in zip(out, ref):
         assert_parity(o, r, rel=1e-5, mabs=1e-4)
+
+
+@pytest.mark.skipif("not __import__('oracle').have_ref_tex()")
+@pytest.mark.parametrize("case", ["small", "motion"])
+def test_warp_invert_vs_reference_texture_kernel(cuda, oracle_lib, case):
+    """nefct_warp_invert against the reference's own DeformInvertKernel
+    (deform_tex.cu.cc:78-99, run on this GPU through its texture units).
+    Both iterate the same 30 Gauss-Seidel passes from 0 with clamp-to-edge
+    trilinear sampling at the same points; the texture unit keeps 8
+    fractional bits of each interpolation weight, this library samples in
+    FP32.  A weight quantised by <= 2^-8 moves a sample by <= 2^-8 x the
+    largest difference of neighbouring field values (here <= 0.6 voxel, so
+    <= 0.0025 voxel), and the contraction (|grad m| <= 0.6) amplifies it by
+    <= 1 / (1 - 0.6): the two inverses may differ by up to ~0.006 voxel
+    (measured on B200: at most 5.7e-3 voxel, 5.2e-4 on average).  The bound
+    asserted is 0.015 voxel at any voxel and 0.002 voxel on average; the
+    same field shifted by one voxel moves the inverse by 0.8-0.9 voxel."""
+    rng = np.random.default_rng(31 if case == "small" else 32)
+    shape = (18, 20, 22) if case == "small" else (40, 48, 56)
+    z, y, x = np.meshgrid(*[np.arange(n, dtype=np.float64) for n in shape], indexing="ij")
+    amp, lam = (1.6, 22.0) if case == "small" else (5.0, 56.0)
+    m = []
+    for _ in range(3):
+        a, ph = rng.uniform(0.5, 1.0) * amp, rng.uniform(0, 2 * np.pi, 3)
+        m.append((a * np.sin(2 * np.pi * x / lam + ph[0]) * np.cos(2 * np.pi * y / lam + ph[1])
+                  + 0.5 * a * np.sin(2 * np.pi * z / lam + ph[2])).astype(np.float32))
+    dm = [torch.from_numpy(a).to(cuda) for a in m]
+    ours = ops.warp_invert(*dm, iters=30)
+    ref = oracle_lib.ref_tex_invert(*dm)
+    torch.cuda.synchronize()
+    for o, r, f in zip(ours, ref, dm):
+        d = (o - r).abs()
+        assert float(r.abs().max()) > 0.3 * float(f.abs().max())       # a real inverse, not zeros
+        assert float(d.max()) <= 0.015, float(d.max())
+        assert float(d.mean()) <= 0.002, float(d.mean())

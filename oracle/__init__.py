@@ -14,6 +14,10 @@ Two layers:
   host C++ from the reference sources (``ref_shim.cc``, ``Makefile``).  Used to
   pin the restatement and as the "reference" CPU baseline.  Present only when
   it was built (it needs the reference checkout at build time).
+* ``_ref/libnefct_ref_gpu.so`` -- the reference's siddon_3d flat-detector
+  kernels and host launchers (``siddon.cu.cc``) compiled by nvcc for the GPU
+  (``ref_gpu_shim.cu``): the reference's own CUDA path, run on device buffers
+  for parity and for timing beside the library.
 * ``_ref/libnefct_ref_tex.so`` -- the reference's texture-based DVF inversion
   (``deform_tex.cu.cc``) compiled by nvcc for the GPU (``ref_tex_shim.cu``):
   hardware texture filtering has no host form, so this one checker runs on
@@ -33,6 +37,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(HERE, "liboracle.so")
 _REF = os.path.join(HERE, "_ref", "libnefct_ref.so")
 _REF_TEX = os.path.join(HERE, "_ref", "libnefct_ref_tex.so")
+_REF_GPU = os.path.join(HERE, "_ref", "libnefct_ref_gpu.so")
 
 TIE_GE, SKIP_SHORT, INV_L2, Q5_TRIPLE_L = 1, 2, 4, 8
 CB_FWD = TIE_GE | INV_L2
@@ -76,6 +81,52 @@ def have_ref() -> bool:
 
 def have_ref_tex() -> bool:
     return os.path.exists(_REF_TEX)
+
+
+def have_ref_gpu() -> bool:
+    return os.path.exists(_REF_GPU)
+
+
+_ref_gpu = None
+
+
+def _ref_gpu_lib():
+    global _ref_gpu
+    if _ref_gpu is None:
+        if not os.path.exists(_REF_GPU):
+            raise FileNotFoundError("oracle/_ref/libnefct_ref_gpu.so was not built")
+        _ref_gpu = C.CDLL(_REF_GPU)
+        args = ([C.c_void_p] + [C.c_int] * 3 + [C.c_float] * 6 + [C.c_void_p] + [C.c_int] * 3 + [C.c_float] * 6
+                + [C.c_void_p])
+        for name in ("ref_gpu_project_flat", "ref_gpu_backproject_flat"):
+            fn = getattr(_ref_gpu, name)
+            fn.restype = C.c_int
+            fn.argtypes = args
+    return _ref_gpu
+
+
+def ref_gpu_cb(forward: bool, g: Grid, x, angles, SID, SAD, na, da, ai, nb, db, bi, out=None):
+    """The reference's own CUDA cone-beam pair (flat detector) on the GPU:
+    ProjectFlatKernel through project_flat (siddon.cu.cc:323-356, 392-420),
+    or BackProjectFlatKernel through backproject_flat (:766-832, 834-862),
+    launched as the reference launches them (16 x 16 x 4 threads, legacy
+    default stream).  x: contiguous float32 CUDA tensor, the volume [nz][ny][nx]
+    (forward) or the sinogram [nv][nb][na] (backprojection); angles: float32
+    CUDA tensor [nv].  The backprojection accumulates into ``out`` (zeroed
+    here when not given), as the reference's atomics do.  Synchronises."""
+    import torch
+    lib_ = _ref_gpu_lib()
+    assert x.is_cuda and x.dtype == torch.float32 and x.is_contiguous()
+    nv = int(angles.numel())
+    if out is None:
+        shape = (nv, nb, na) if forward else (g.nz, g.ny, g.nx)
+        out = torch.zeros(shape, dtype=torch.float32, device=x.device)
+    fn = lib_.ref_gpu_project_flat if forward else lib_.ref_gpu_backproject_flat
+    err = fn(x.data_ptr(), g.nx, g.ny, g.nz, g.cx, g.cy, g.cz, g.sx, g.sy, g.sz,
+             angles.contiguous().data_ptr(), na, nb, nv, SID, SAD, da, ai, db, bi, out.data_ptr())
+    if err:
+        raise RuntimeError(f"reference CUDA {'forward' if forward else 'backprojection'} failed: CUDA error {err}")
+    return out
 
 
 _ref_tex = None

@@ -446,9 +446,79 @@ struct BpParams {
 // When |m/db| * max|z| + |nb/2 - bi - 0.5| could reach 2^21 (a voxel at or
 // near the source plane has an infinite or NaN b) the thread clamps b to
 // [-2, nb + 1] first.  The distance weight is folded into the column
-// weights (wa u, wa2 u) once per view.
+// weights (wa u, wa2 u) once per view.  Every operation is written with its
+// rounding (no contraction left to the compiler), so fdk_edge_kernel
+// recomputes the same values.
 // QUAD: the taps come from the chunk's tap quads (fdk_quad_kernel) with one
 // 16-byte load; the arithmetic is the same, so are the results, bit for bit.
+
+// Column part of one view for the voxel column at (xc, yc): bp_column the
+// detector column (a, ia) and the magnification, bp_weights (for a column
+// that is kept) the row slope bm and the column weights.
+struct BpColumn {
+    float a, bm, wau, wa2u;
+    float inv, m;
+    int ia;
+};
+
+__device__ __forceinline__ void bp_column(const BpParams &p, float cphi, float sphi, float xc, float yc, BpColumn &c)
+{
+    const float xc0 = __fmaf_rn(xc, cphi, __fmul_rn(yc, sphi));
+    const float yc0 = __fmaf_rn(-xc, sphi, __fmul_rn(yc, cphi));
+    const float nah = (float)(p.na / 2);                   // integer half (Q9)
+    // 1 / (xc0 - xs) = 1 / (src_iso + xc0): magnification and distance weight share it
+    c.inv = rcp_approx(__fadd_rn(xc0, p.src_iso));
+    c.m = __fmul_rn(p.src_det, c.inv);                     // SAD / (xc0 - xs)
+    float t;
+    if (p.cyl) t = __fmaf_rn(atan2f(yc0, __fadd_rn(xc0, p.src_iso)), p.inv_da, nah);
+    else t = __fmaf_rn(__fmul_rn(c.m, yc0), p.inv_da, nah);
+    c.a = __fsub_rn(__fsub_rn(t, p.ai_p), 0.5f);
+    c.ia = __float2int_rd(c.a);
+}
+
+__device__ __forceinline__ void bp_weights(const BpParams &p, BpColumn &c)
+{
+    c.bm = __fmul_rn(c.m, p.inv_db);
+    float u = 1.f;
+    if (p.weight) {
+        const float r = __fmul_rn(p.src_iso, c.inv);
+        u = __fmul_rn(r, r);
+    }
+    const float wa2 = __fsub_rn(c.a, (float)c.ia), wa = __fsub_rn(1.f, wa2);
+    c.wau = __fmul_rn(wa, u);
+    c.wa2u = __fmul_rn(wa2, u);
+}
+
+// Voxel centre along one axis, pixel.cu.cc:116-118 ((i + 0.5) * s / n + c, in double).
+__device__ __forceinline__ float bp_centre(int i, float s, int n, float c)
+{
+    return (float)((i + 0.5) * (double)s / n + (double)c);
+}
+
+// Contribution of one voxel at detector row b from the column's taps:
+// false when Q11 drops it (ib < 0 || ib + 1 >= nb).
+template <bool QUAD>
+__device__ __forceinline__ bool bp_tap(const BpParams &p, const float *pv, const float4 *pq, const BpColumn &c, float b,
+                                       float &r0, float &r1, float &wb, float &wb2)
+{
+    const float mb = __fadd_rd(b, 12582912.0f);
+    const unsigned ib = (unsigned)(__float_as_int(mb) - 0x4B400000);
+    if (ib >= (unsigned)(p.nb - 1)) return false;
+    wb2 = __fsub_rn(b, __fsub_rn(mb, 12582912.0f));
+    wb = __fsub_rn(1.f, wb2);
+    float t00, t01, t10, t11;
+    if (QUAD) {
+        const float4 q4 = __ldg(pq + (size_t)ib * p.na);
+        t00 = q4.x; t01 = q4.y; t10 = q4.z; t11 = q4.w;
+    } else {
+        const float *q = pv + (size_t)ib * p.na;
+        t00 = __ldg(q); t01 = __ldg(q + 1); t10 = __ldg(q + p.na); t11 = __ldg(q + p.na + 1);
+    }
+    r0 = __fmaf_rn(t01, c.wa2u, __fmul_rn(t00, c.wau));
+    r1 = __fmaf_rn(t11, c.wa2u, __fmul_rn(t10, c.wau));
+    return true;
+}
+
 template <bool QUAD>
 __global__ void __launch_bounds__(128) fdk_bp_kernel(const __grid_constant__ BpParams p,
                                                      const float *__restrict__ sino, const float4 *__restrict__ quad,
@@ -458,86 +528,39 @@ __global__ void __launch_bounds__(128) fdk_bp_kernel(const __grid_constant__ BpP
     const int iy = (blockIdx.y * 4 + threadIdx.y) * (32 / kTW) + threadIdx.x / kTW;
     const int z0 = blockIdx.z * kZ;
     if (ix >= p.nx || iy >= p.ny) return;
-    // voxel centres, pixel.cu.cc:116-118 ((ix + 0.5) * sx / nx + cx, in double)
-    const float xc = (float)((ix + 0.5) * (double)p.sx / p.nx + (double)p.corner_x);
-    const float yc = (float)((iy + 0.5) * (double)p.sy / p.ny + (double)p.corner_y);
+    const float xc = bp_centre(ix, p.sx, p.nx, p.corner_x);
+    const float yc = bp_centre(iy, p.sy, p.ny, p.corner_y);
     float zc[kZ], acc[kZ];
     const size_t plane = (size_t)p.nx * p.ny;
     const size_t col = (size_t)iy * p.nx + ix;
 #pragma unroll
     for (int k = 0; k < kZ; ++k) {
         const int iz = z0 + k;
-        zc[k] = (float)((iz + 0.5) * (double)p.sz / p.nz + (double)p.corner_z);
+        zc[k] = bp_centre(iz, p.sz, p.nz, p.corner_z);
         acc[k] = (!p.first && iz < p.nz) ? vol[iz * plane + col] : 0.f;
     }
     float zabs = 0.f;
 #pragma unroll
     for (int k = 0; k < kZ; ++k) zabs = fmaxf(zabs, fabsf(zc[k]));
-    const float xs = -p.src_iso;
-    const float nah = (float)(p.na / 2);   // integer half (Q9)
     const float bhi = (float)(p.nb + 1);
-    const unsigned nb1 = (unsigned)(p.nb - 1);
     for (int v = 0; v < p.nvc; ++v) {
-        const float cphi = p.cs[v], sphi = p.sn[v];
-        const float xc0 = xc * cphi + yc * sphi;
-        const float yc0 = -xc * sphi + yc * cphi;
-        // 1 / (xc0 - xs) = 1 / (src_iso + xc0): magnification and distance weight share it
-        const float inv = rcp_approx(xc0 - xs);
-        const float m = p.src_det * inv;                       // SAD / (xc0 - xs)
-        float t;
-        if (p.cyl) t = atan2f(yc0, xc0 + p.src_iso) * p.inv_da + nah;
-        else t = m * yc0 * p.inv_da + nah;
-        const float a = __fsub_rn(__fsub_rn(t, p.ai_p), 0.5f);
-        const int ia = __float2int_rd(a);
-        if (ia < 0 || ia + 1 >= p.na) continue;               // Q11
-        const float wa2 = a - (float)ia, wa = 1.f - wa2;
-        float u = 1.f;
-        if (p.weight) {
-            const float r = p.src_iso * inv;
-            u = r * r;
-        }
-        const float bm = m * p.inv_db;
-        const float wau = wa * u, wa2u = wa2 * u;
-        const float *pv = sino + (size_t)v * p.na * p.nb + ia;
-        const float4 *pq = QUAD ? quad + (size_t)v * p.na * p.nb + ia : nullptr;
-        // the 2 x 2 taps of detector row ib (rows ib and ib + 1, columns ia, ia + 1)
-        auto taps = [&](unsigned ib, float &t00, float &t01, float &t10, float &t11) {
-            if (QUAD) {
-                const float4 q4 = __ldg(pq + (size_t)ib * p.na);
-                t00 = q4.x; t01 = q4.y; t10 = q4.z; t11 = q4.w;
-            } else {
-                const float *q = pv + (size_t)ib * p.na;
-                t00 = __ldg(q); t01 = __ldg(q + 1); t10 = __ldg(q + p.na); t11 = __ldg(q + p.na + 1);
-            }
-        };
-        if (fabsf(bm) * zabs + fabsf(p.cb) < 2097152.f) {
+        BpColumn c;
+        bp_column(p, p.cs[v], p.sn[v], xc, yc, c);
+        if (c.ia < 0 || c.ia + 1 >= p.na) continue;             // Q11
+        bp_weights(p, c);
+        const float *pv = sino + (size_t)v * p.na * p.nb + c.ia;
+        const float4 *pq = QUAD ? quad + (size_t)v * p.na * p.nb + c.ia : nullptr;
+        float r0, r1, wb, wb2;
+        if (fabsf(c.bm) * zabs + fabsf(p.cb) < 2097152.f) {
 #pragma unroll
-            for (int k = 0; k < kZ; ++k) {
-                const float b = fmaf(bm, zc[k], p.cb);
-                const float mb = __fadd_rd(b, 12582912.0f);
-                const unsigned ib = (unsigned)(__float_as_int(mb) - 0x4B400000);
-                if (ib >= nb1) continue;
-                const float wb2 = b - __fsub_rn(mb, 12582912.0f), wb = 1.f - wb2;
-                float t00, t01, t10, t11;
-                taps(ib, t00, t01, t10, t11);
-                const float r0 = fmaf(t01, wa2u, t00 * wau);
-                const float r1 = fmaf(t11, wa2u, t10 * wau);
-                acc[k] = fmaf(r1, wb2, fmaf(r0, wb, acc[k]));
-            }
+            for (int k = 0; k < kZ; ++k)
+                if (bp_tap<QUAD>(p, pv, pq, c, __fmaf_rn(c.bm, zc[k], p.cb), r0, r1, wb, wb2))
+                    acc[k] = __fmaf_rn(r1, wb2, __fmaf_rn(r0, wb, acc[k]));
         } else {
 #pragma unroll
-            for (int k = 0; k < kZ; ++k) {
-                const float b = fminf(fmaxf(fmaf(bm, zc[k], p.cb), -2.f), bhi);
-                const float mb = __fadd_rd(b, 12582912.0f);
-                const unsigned ib = (unsigned)(__float_as_int(mb) - 0x4B400000);
-                if (ib >= nb1) continue;                           // ib < 0 || ib + 1 >= nb
-                const float wb2 = b - __fsub_rn(mb, 12582912.0f), wb = 1.f - wb2;
-                float t00, t01, t10, t11;
-                taps(ib, t00, t01, t10, t11);
-                const float r0 = fmaf(t01, wa2u, t00 * wau);
-                const float r1 = fmaf(t11, wa2u, t10 * wau);
-                acc[k] = fmaf(r1, wb2, fmaf(r0, wb, acc[k]));
-            }
+            for (int k = 0; k < kZ; ++k)
+                if (bp_tap<QUAD>(p, pv, pq, c, fminf(fmaxf(__fmaf_rn(c.bm, zc[k], p.cb), -2.f), bhi), r0, r1, wb, wb2))
+                    acc[k] = __fmaf_rn(r1, wb2, __fmaf_rn(r0, wb, acc[k]));
         }
     }
 #pragma unroll
@@ -545,6 +568,187 @@ __global__ void __launch_bounds__(128) fdk_bp_kernel(const __grid_constant__ BpP
         if (z0 + k < p.nz) vol[(z0 + k) * plane + col] = acc[k];
 }
 
+// ---- detector-edge decisions with the reference's own operations ----
+//
+// The few-ulp differences above move the bilinear weights continuously
+// everywhere except at the detector's edges, where the reference drops a
+// voxel whose tap pair reaches past the last column or row, or starts before
+// the first (Q11): there a row or column within ulps of the edge can be kept
+// by one evaluation and dropped by the other.  For a flat detector,
+// fdk_edge_kernel revisits, after fdk_bp_kernel, every (column, view) of the
+// chunk whose detector column lies within `edge` of column 0 or na - 1, and
+// every voxel whose row lies within `edge` of row 0 or nb - 1; it decides
+// each with the reference's operations in order (pixel.cu.cc:24-33, no
+// contraction: exact_col, exact_row) and takes a voxel the kernel kept and
+// the reference drops out of the sum, or puts one the reference keeps in.
+
+// pixel.cu.cc:24-29: the rotated voxel centre and the magnification
+// SAD / (x' - xs) (xs = -src_iso).
+__device__ __forceinline__ float exact_mag(const BpParams &p, float cphi, float sphi, float xc, float yc, float &yr)
+{
+    const float xr = __fadd_rn(__fmul_rn(xc, cphi), __fmul_rn(yc, sphi));
+    yr = __fadd_rn(__fmul_rn(-xc, sphi), __fmul_rn(yc, cphi));
+    return __fdiv_rn(p.src_det, __fadd_rn(xr, p.src_iso));
+}
+
+// pixel.cu.cc:30-32: a = yd / da + na / 2 - ai - 0.5 (the last subtraction
+// in double, rounded to float: the same as the float subtraction).
+__device__ __forceinline__ float exact_col(const BpParams &p, float cphi, float sphi, float xc, float yc)
+{
+    float yr;
+    const float m = exact_mag(p, cphi, sphi, xc, yc, yr);
+    return __fsub_rn(__fsub_rn(__fadd_rn(__fdiv_rn(__fmul_rn(m, yr), p.da), (float)(p.na / 2)), p.ai_p), 0.5f);
+}
+
+// pixel.cu.cc:28,31: b = (SAD / (x' - xs)) * z / db + nb / 2 - bi - 0.5.
+__device__ __forceinline__ float exact_row(const BpParams &p, float cphi, float sphi, float xc, float yc, float zc)
+{
+    float yr;
+    const float m = exact_mag(p, cphi, sphi, xc, yc, yr);
+    return __fsub_rn(__fsub_rn(__fadd_rn(__fdiv_rn(__fmul_rn(m, zc), p.db), (float)(p.nb / 2)), p.bi_p), 0.5f);
+}
+
+// Column (row) decisions: kept when 0 <= floor(x) and floor(x) + 1 < n.
+__device__ __forceinline__ bool bp_keep(float x, int n)
+{
+    const int i = __float2int_rd(x);
+    return i >= 0 && i + 1 < n;
+}
+
+// One warp per voxel column; lane l takes views l, l + 32, ... of one table
+// (up to kViewChunk views, after every chunk's backprojection) and finds, in
+// parallel, the voxels whose decisions differ and the corrections; the
+// corrections are then applied by one lane at a time in view order, so the
+// result stays deterministic (and the same with and without tap quads: the
+// taps are read from the filtered sinogram, which the quads copy).
+static constexpr int kEdgeSlots = 4;
+
+__global__ void __launch_bounds__(256) fdk_edge_kernel(const __grid_constant__ BpParams p,
+                                                       const float *__restrict__ sino, float *vol)
+{
+    const int lane = threadIdx.x & 31;
+    const long long colid = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (colid >= (long long)p.nx * p.ny) return;           // uniform across the warp
+    const int ix = (int)(colid % p.nx), iy = (int)(colid / p.nx);
+    const float xc = bp_centre(ix, p.sx, p.nx, p.corner_x);
+    const float yc = bp_centre(iy, p.sy, p.ny, p.corner_y);
+    const float naf = (float)p.na, nbf = (float)p.nb;
+    const float edge = 1.f / 64 + fmaxf(naf, nbf) * (1.f / 16384);   // >> the few-ulp differences
+    const size_t plane = (size_t)p.nx * p.ny;
+    float *const vcol = vol + (size_t)iy * p.nx + ix;
+    const float idz = (float)p.nz / p.sz;
+    const float z_first = bp_centre(0, p.sz, p.nz, p.corner_z), z_last = bp_centre(p.nz - 1, p.sz, p.nz, p.corner_z);
+    for (int v0 = 0; v0 < p.nvc; v0 += 32) {
+        const int v = v0 + lane;
+        const bool has = v < p.nvc;
+        const int vt = min(v, p.nvc - 1);                  // lanes past the table read its last entry
+        const float cphi = p.cs[vt], sphi = p.sn[vt];
+        BpColumn c, cr;
+        bool col_ours = false, col_ref = false;
+        if (has) {
+            bp_column(p, cphi, sphi, xc, yc, c);
+            bp_weights(p, c);
+            col_ours = c.ia >= 0 && c.ia + 1 < p.na;
+            col_ref = col_ours;
+            cr = c;                           // the column as the reference places it
+            if (!p.cyl && (fabsf(c.a) < edge || fabsf(c.a - (naf - 1.f)) < edge)) {
+                cr.a = exact_col(p, cphi, sphi, xc, yc);
+                cr.ia = __float2int_rd(cr.a);
+                col_ref = cr.ia >= 0 && cr.ia + 1 < p.na;
+                const float wa2 = __fsub_rn(cr.a, (float)cr.ia);
+                const float u = __fadd_rn(c.wau, c.wa2u);     // the distance weight (wa + wa2 = 1)
+                cr.wau = __fmul_rn(__fsub_rn(1.f, wa2), u);
+                cr.wa2u = __fmul_rn(wa2, u);
+            }
+        }
+        const size_t off = (size_t)v * p.na * p.nb;
+        auto contribution = [&](const BpColumn &cc, float b, float &out) -> bool {
+            float r0, r1, wb, wb2;
+            if (!bp_tap<false>(p, sino + off + cc.ia, nullptr, cc, b, r0, r1, wb, wb2)) return false;
+            out = __fmaf_rn(r1, wb2, __fmul_rn(r0, wb));
+            return true;
+        };
+        // correction of voxel iz (0 where the decisions agree)
+        auto delta = [&](int iz, bool whole_column) -> float {
+            const float zc = bp_centre(iz, p.sz, p.nz, p.corner_z);
+            const float b = __fmaf_rn(c.bm, zc, p.cb);
+            const bool near_row = fabsf(b) < edge || fabsf(b - (nbf - 1.f)) < edge;
+            if (!whole_column && !near_row) return 0.f;
+            const float br = near_row ? exact_row(p, cphi, sphi, xc, yc, zc) : b;
+            float co = 0.f, cref = 0.f;
+            const bool ours = col_ours && bp_keep(b, p.nb) && contribution(c, b, co);
+            const bool ref = col_ref && bp_keep(br, p.nb) && contribution(cr, br, cref);
+            if (ours == ref && !whole_column) return 0.f;
+            return __fsub_rn(ref ? cref : 0.f, ours ? co : 0.f);
+        };
+        // voxel range of the band of rows within `edge` of row 0 (e = 0) or
+        // nb - 1 (e = 1): the rows are monotone in z (b = bm z + cb), so the
+        // band is one z interval, mapped to voxel indices in float with a
+        // margin of 1/64 voxel (its rounding is ~1e-4 voxel); the band is
+        // ~0.1 voxel wide, so most (column, view) pairs have no candidate
+        float b_first = 0.f, b_last = 0.f, ibm = 0.f;
+        auto band = [&](int e, int &i0, int &i1) {
+            const float target = e ? nbf - 1.f : 0.f;
+            const float za = (target - edge - p.cb) * ibm, zb = (target + edge - p.cb) * ibm;
+            const float flo = (fminf(za, zb) - p.corner_z) * idz - 0.5f - 1.f / 64;
+            const float fhi = (fmaxf(za, zb) - p.corner_z) * idz - 0.5f + 1.f / 64;
+            i0 = max(0, __float2int_ru(fmaxf(flo, -1.f)));
+            i1 = min(p.nz - 1, __float2int_rd(fminf(fhi, (float)p.nz)));
+        };
+        // rows of the column over the grid's z extent (a little wider): a
+        // band outside it has no voxel
+        auto reaches = [&](int e) {
+            const float target = e ? nbf - 1.f : 0.f;
+            return fminf(b_first, b_last) - 1.f < target && target < fmaxf(b_first, b_last) + 1.f;
+        };
+        int n = 0, slot_iz[kEdgeSlots];
+        float slot_d[kEdgeSlots];
+        bool serial = has && col_ours != col_ref;   // the whole column differs: done one lane at a time
+        if (has && !serial && col_ours && c.bm != 0.f) {
+            b_first = __fmaf_rn(c.bm, z_first, p.cb);
+            b_last = __fmaf_rn(c.bm, z_last, p.cb);
+            ibm = rcp_approx(c.bm);
+            for (int e = 0; e < 2; ++e) {
+                if (!reaches(e)) continue;
+                int i0, i1;
+                band(e, i0, i1);
+                for (int iz = i0; iz <= i1; ++iz) {
+                    const float d = delta(iz, false);
+                    if (d == 0.f) continue;
+                    if (n < kEdgeSlots) { slot_iz[n] = iz; slot_d[n] = d; ++n; }
+                    else serial = true;
+                }
+            }
+        }
+        // apply in view order: lane by lane
+        unsigned pending = __ballot_sync(0xffffffffu, n > 0 || serial);
+        while (pending) {
+            const int src = __ffs(pending) - 1;
+            pending &= pending - 1;
+            if (lane == src) {
+                if (col_ours != col_ref) {
+                    for (int iz = 0; iz < p.nz; ++iz) {
+                        const float d = delta(iz, true);
+                        if (d != 0.f) vcol[(size_t)iz * plane] = __fadd_rn(vcol[(size_t)iz * plane], d);
+                    }
+                } else if (serial) {                   // more corrections than slots (rare)
+                    for (int e = 0; e < 2; ++e) {
+                        int i0, i1;
+                        band(e, i0, i1);
+                        for (int iz = i0; iz <= i1; ++iz) {
+                            const float d = delta(iz, false);
+                            if (d != 0.f) vcol[(size_t)iz * plane] = __fadd_rn(vcol[(size_t)iz * plane], d);
+                        }
+                    }
+                } else {
+                    for (int k = 0; k < n; ++k)
+                        vcol[(size_t)slot_iz[k] * plane] = __fadd_rn(vcol[(size_t)slot_iz[k] * plane], slot_d[k]);
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
 }  // namespace nefct
 
 using namespace nefct;
@@ -675,6 +879,20 @@ nefct_status nefct_fdk_backproject_ws(const nefct_cb_geom *g, const float *filte
         }
         e = cudaGetLastError();
         if (e != cudaSuccess) { delete p; return cuda_fail(e, "fdk_bp_kernel"); }
+    }
+    // detector-edge decisions, a warp per voxel column, kViewChunk views per launch
+    const long long columns = (long long)g->grid.nx * g->grid.ny;
+    const unsigned eblocks = (unsigned)((columns + 7) / 8);        // a warp per column
+    for (int v0 = 0; v0 < g->nv; v0 += kViewChunk) {
+        p->nv0 = v0;
+        p->nvc = std::min(kViewChunk, g->nv - v0);
+        for (int i = 0; i < p->nvc; ++i) {
+            p->cs[i] = (float)cos((double)g->angles[v0 + i]);
+            p->sn[i] = (float)sin((double)g->angles[v0 + i]);
+        }
+        fdk_edge_kernel<<<eblocks, 256, 0, s>>>(*p, filtered + (size_t)v0 * g->na * g->nb, vol);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) { delete p; return cuda_fail(e, "fdk_edge_kernel"); }
     }
     delete p;
     return NEFCT_OK;

@@ -15,9 +15,10 @@ Two layers:
   pin the restatement and as the "reference" CPU baseline.  Present only when
   it was built (it needs the reference checkout at build time).
 * ``_ref/libnefct_ref_gpu.so`` -- the reference's siddon_3d flat-detector
-  kernels and host launchers (``siddon.cu.cc``) compiled by nvcc for the GPU
-  (``ref_gpu_shim.cu``): the reference's own CUDA path, run on device buffers
-  for parity and for timing beside the library.
+  pair, pixel_3d backprojection and cpp/siddon LOR pair with their host
+  launchers, compiled by nvcc for the GPU (``ref_gpu_shim.cu``): the
+  reference's own CUDA path, run on device buffers for parity and for timing
+  beside the library.
 * ``_ref/libnefct_ref_tex.so`` -- the reference's texture-based DVF inversion
   (``deform_tex.cu.cc``) compiled by nvcc for the GPU (``ref_tex_shim.cu``):
   hardware texture filtering has no host form, so this one checker runs on
@@ -98,11 +99,63 @@ def _ref_gpu_lib():
         _ref_gpu = C.CDLL(_REF_GPU)
         args = ([C.c_void_p] + [C.c_int] * 3 + [C.c_float] * 6 + [C.c_void_p] + [C.c_int] * 3 + [C.c_float] * 6
                 + [C.c_void_p])
-        for name in ("ref_gpu_project_flat", "ref_gpu_backproject_flat"):
+        for name in ("ref_gpu_project_flat", "ref_gpu_backproject_flat", "ref_gpu_pixel_backproject_flat"):
             fn = getattr(_ref_gpu, name)
             fn.restype = C.c_int
             fn.argtypes = args
+        lor_args = [C.c_void_p] + [C.c_int] * 4 + [C.c_float] * 6 + [C.c_void_p] * 2
+        for name in ("ref_gpu_lor_forward", "ref_gpu_lor_backward"):
+            fn = getattr(_ref_gpu, name)
+            fn.restype = C.c_int
+            fn.argtypes = lor_args
     return _ref_gpu
+
+
+def _check_gpu(err, what):
+    if err:
+        raise RuntimeError(f"reference CUDA {what} failed: CUDA error {err}")
+
+
+def ref_gpu_pixel_backproject(sino, shape, corner, size, angles, SID, SAD, na, da, ai, nb, db, bi):
+    """The reference's pixel_3d BackProjectFlatKernel through backproject_flat
+    (pixel.cu.cc:98-175) on the GPU.  sino: float32 CUDA tensor
+    [nv][nb][na]; shape (nx, ny, nz), corner = the grid's low corner (Q10),
+    size in mm; returns the volume [nz][ny][nx].  Synchronises."""
+    import torch
+    lib_ = _ref_gpu_lib()
+    assert sino.is_cuda and sino.dtype == torch.float32 and sino.is_contiguous()
+    nx, ny, nz = shape
+    out = torch.zeros((nz, ny, nx), dtype=torch.float32, device=sino.device)
+    _check_gpu(lib_.ref_gpu_pixel_backproject_flat(sino.data_ptr(), nx, ny, nz, *corner, *size,
+                                                  angles.contiguous().data_ptr(), na, nb, int(angles.numel()),
+                                                  SID, SAD, da, ai, db, bi, out.data_ptr()),
+               "pixel_3d backprojection")
+    return out
+
+
+def ref_gpu_lor(forward: bool, lors, shape, center, size, x):
+    """The reference's cpp/siddon ProjectKernel / BackProjectKernel through
+    projection / backprojection (siddon_gpu.cu.cc:652-747), launched as the
+    reference launches them (32 CTAs of 1024 threads).  lors: float32 CUDA
+    tensor [6][n]; x: the volume [nz][ny][nx] (forward) or the line values [n]
+    (backprojection).  Outputs are zeroed first (the reference leaves skipped
+    lines unwritten, Q4, and accumulates into an unzeroed volume, Q6).
+    Synchronises."""
+    import torch
+    lib_ = _ref_gpu_lib()
+    assert lors.is_cuda and lors.dtype == torch.float32 and lors.is_contiguous() and lors.shape[0] == 6
+    n = int(lors.shape[1])
+    nx, ny, nz = shape
+    if forward:
+        out = torch.zeros(n, dtype=torch.float32, device=lors.device)
+        err = lib_.ref_gpu_lor_forward(lors.data_ptr(), n, nx, ny, nz, *center, *size, x.contiguous().data_ptr(),
+                                       out.data_ptr())
+    else:
+        out = torch.zeros((nz, ny, nx), dtype=torch.float32, device=lors.device)
+        err = lib_.ref_gpu_lor_backward(lors.data_ptr(), n, nx, ny, nz, *center, *size, x.contiguous().data_ptr(),
+                                        out.data_ptr())
+    _check_gpu(err, "LOR " + ("forward" if forward else "backprojection"))
+    return out
 
 
 def ref_gpu_cb(forward: bool, g: Grid, x, angles, SID, SAD, na, da, ai, nb, db, bi, out=None):
@@ -124,8 +177,7 @@ def ref_gpu_cb(forward: bool, g: Grid, x, angles, SID, SAD, na, da, ai, nb, db, 
     fn = lib_.ref_gpu_project_flat if forward else lib_.ref_gpu_backproject_flat
     err = fn(x.data_ptr(), g.nx, g.ny, g.nz, g.cx, g.cy, g.cz, g.sx, g.sy, g.sz,
              angles.contiguous().data_ptr(), na, nb, nv, SID, SAD, da, ai, db, bi, out.data_ptr())
-    if err:
-        raise RuntimeError(f"reference CUDA {'forward' if forward else 'backprojection'} failed: CUDA error {err}")
+    _check_gpu(err, "forward" if forward else "backprojection")
     return out
 
 

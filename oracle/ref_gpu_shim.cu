@@ -1,19 +1,37 @@
-// TEST INFRASTRUCTURE: the reference's siddon_3d cone-beam kernels and their
-// host launchers (nefct/cc/siddon_3d/siddon.cu.cc:6-890: project_device,
-// ProjectFlatKernel, project_flat, backproject_device, BackProjectFlatKernel,
-// backproject_flat, ...) built unchanged by nvcc from the reference checkout
-// (the Makefile extracts the line range into _ref/gen/siddon3d_gpu.inc).  It
-// runs the reference's own CUDA path on the GPU for the parity tests and for
+// TEST INFRASTRUCTURE: the reference's own CUDA kernels and their host
+// launchers, built unchanged by nvcc from the reference checkout (the
+// Makefile extracts the line ranges into _ref/gen/):
+//   siddon3d_gpu.inc  nefct/cc/siddon_3d/siddon.cu.cc:6-890 (cone-beam pair)
+//   pixel3d_gpu.inc   nefct/cc/pixel_3d/pixel.cu.cc:6-204 (voxel-driven
+//                     backprojection)
+//   lor_gpu.inc       cpp/siddon/siddon_gpu.cu.cc:6-747 (LOR pair)
+// Each file sits in its own namespace (they share function names).  It runs
+// the reference's own CUDA path on the GPU for the parity tests and for
 // timing that path beside the library's.  Only tests load it.
 //
-// The flat-detector kernels index the volume only under their own range
-// checks (every image access and atomicAdd sits behind 0 <= c < n tests of
-// its indices, and the sinogram index ia + ib*na + iv*na*nb stays below
-// na*nb*nv); the cylindrical backprojection's sinogram index (quirk Q8,
-// :830) can leave the buffer when nb > nv, so only the flat pair is exported.
+// Read before running: every volume access and atomicAdd of these kernels
+// sits behind range checks of its indices (0 <= c < n, with the neighbour
+// index checked on its open side); pixel_3d reads its four taps only when
+// ia >= 0, ia + 1 < na, ib >= 0, ib + 1 < nb; the flat sinogram index
+// ia + ib*na + iv*na*nb and the LOR index tid < num_events stay in their
+// buffers.  The cylindrical siddon_3d backprojection reads its sinogram at
+// ia + iv*na + ib*na*nb (quirk Q8, siddon.cu.cc:830), which leaves the
+// buffer when nb > nv, so only the flat variants are exported.
 #include <cuda_runtime.h>
+#include <stddef.h>
 
+namespace s3d {
 #include "siddon3d_gpu.inc"
+}
+#undef abs
+namespace px3 {
+#include "pixel3d_gpu.inc"
+}
+#undef abs
+namespace lor {
+#include "lor_gpu.inc"
+}
+#undef abs
 
 namespace {
 
@@ -24,21 +42,18 @@ struct HostGrid {
 };
 
 // The reference's host functions read grid / center / size back from the
-// device (siddon.cu.cc:401-406), so they are staged in one device block.
-// Runs on the legacy default stream like the reference and synchronises.
-int run(bool forward, const float *in, const HostGrid &hg, const float *angles, int na, int nb, int nv, float SID,
-        float SAD, float da, float ai, float db, float bi, float *out)
+// device (e.g. siddon.cu.cc:401-406), so they are staged in one device block.
+// Everything runs on the legacy default stream like the reference; the
+// call synchronises and returns the CUDA error code (0 = success).
+template <class Fn> int with_grid(const HostGrid &hg, Fn fn)
 {
     unsigned char *blk = nullptr;
     cudaError_t e = cudaMalloc(&blk, sizeof(HostGrid));
     if (e != cudaSuccess) return (int)e;
     e = cudaMemcpy(blk, &hg, sizeof(HostGrid), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
-        const int *grid = (const int *)blk;
-        const float *center = (const float *)(blk + offsetof(HostGrid, center));
-        const float *size = (const float *)(blk + offsetof(HostGrid, size));
-        if (forward) project_flat(in, grid, center, size, angles, na, nb, nv, SID, SAD, da, ai, db, bi, out);
-        else backproject_flat(in, grid, center, size, angles, na, nb, nv, SID, SAD, da, ai, db, bi, out);
+        fn((const int *)blk, (const float *)(blk + offsetof(HostGrid, center)),
+           (const float *)(blk + offsetof(HostGrid, size)));
         e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
     }
@@ -50,24 +65,60 @@ int run(bool forward, const float *in, const HostGrid &hg, const float *angles, 
 
 extern "C" {
 
-// vol: device [nz][ny][nx]; angles: device [nv]; sino: device [nv][nb][na].
-// Geometry in the reference kernels' naming (SID source-isocentre, SAD
-// source-detector).  Returns the CUDA error code (0 = success).
+// siddon_3d flat pair.  vol: device [nz][ny][nx]; angles: device [nv];
+// sino: device [nv][nb][na].  Kernel naming (SID source-isocentre, SAD
+// source-detector), grid given by its centre.  The backprojection
+// accumulates into vol (the reference's atomics; zero it first).
 int ref_gpu_project_flat(const float *vol, int nx, int ny, int nz, float cx, float cy, float cz, float sx, float sy,
                          float sz, const float *angles, int na, int nb, int nv, float SID, float SAD, float da,
                          float ai, float db, float bi, float *sino)
 {
-    const HostGrid hg = {{nx, ny, nz}, {cx, cy, cz}, {sx, sy, sz}};
-    return run(true, vol, hg, angles, na, nb, nv, SID, SAD, da, ai, db, bi, sino);
+    return with_grid({{nx, ny, nz}, {cx, cy, cz}, {sx, sy, sz}}, [&](const int *g, const float *c, const float *s) {
+        s3d::project_flat(vol, g, c, s, angles, na, nb, nv, SID, SAD, da, ai, db, bi, sino);
+    });
 }
 
-// sino -> vol, accumulated into vol (the reference's atomics; zero it first).
 int ref_gpu_backproject_flat(const float *sino, int nx, int ny, int nz, float cx, float cy, float cz, float sx,
                              float sy, float sz, const float *angles, int na, int nb, int nv, float SID, float SAD,
                              float da, float ai, float db, float bi, float *vol)
 {
-    const HostGrid hg = {{nx, ny, nz}, {cx, cy, cz}, {sx, sy, sz}};
-    return run(false, sino, hg, angles, na, nb, nv, SID, SAD, da, ai, db, bi, vol);
+    return with_grid({{nx, ny, nz}, {cx, cy, cz}, {sx, sy, sz}}, [&](const int *g, const float *c, const float *s) {
+        s3d::backproject_flat(sino, g, c, s, angles, na, nb, nv, SID, SAD, da, ai, db, bi, vol);
+    });
+}
+
+// pixel_3d flat backprojection (pixel.cu.cc:148-175): the grid is given by
+// its low corner (quirk Q10); accumulates into vol (zero it first).
+int ref_gpu_pixel_backproject_flat(const float *sino, int nx, int ny, int nz, float x0, float y0, float z0, float sx,
+                                   float sy, float sz, const float *angles, int na, int nb, int nv, float SID,
+                                   float SAD, float da, float ai, float db, float bi, float *vol)
+{
+    return with_grid({{nx, ny, nz}, {x0, y0, z0}, {sx, sy, sz}}, [&](const int *g, const float *c, const float *s) {
+        px3::backproject_flat(sino, g, c, s, angles, na, nb, nv, SID, SAD, da, ai, db, bi, vol);
+    });
+}
+
+// cpp/siddon LOR pair (siddon_gpu.cu.cc:700-747).  lors: device [6][n] rows
+// x1 y1 z1 x2 y2 z2.  The forward writes out[i] except for the lines it
+// skips (quirk Q4: zero out first); the backprojection accumulates into vol
+// (quirk Q6: zero it first).
+int ref_gpu_lor_forward(const float *lors, int n, int nx, int ny, int nz, float cx, float cy, float cz, float sx,
+                        float sy, float sz, const float *vol, float *out)
+{
+    const size_t r = (size_t)n;
+    return with_grid({{nx, ny, nz}, {cx, cy, cz}, {sx, sy, sz}}, [&](const int *g, const float *c, const float *s) {
+        lor::projection(lors, lors + r, lors + 2 * r, lors + 3 * r, lors + 4 * r, lors + 5 * r, out, g, c, s, vol, n);
+    });
+}
+
+int ref_gpu_lor_backward(const float *lors, int n, int nx, int ny, int nz, float cx, float cy, float cz, float sx,
+                         float sy, float sz, const float *vals, float *vol)
+{
+    const size_t r = (size_t)n;
+    return with_grid({{nx, ny, nz}, {cx, cy, cz}, {sx, sy, sz}}, [&](const int *g, const float *c, const float *s) {
+        lor::backprojection(lors, lors + r, lors + 2 * r, lors + 3 * r, lors + 4 * r, lors + 5 * r, vals, g, c, s, vol,
+                            n);
+    });
 }
 
 }  // extern "C"

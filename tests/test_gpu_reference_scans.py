@@ -12,7 +12,9 @@ subsets, against the reference's own projector code built for the host
   reference's own backprojector: the reference's forward weights carry
   1 / L^2 and its backprojection does not (siddon.cu.cc:86 vs :526), so
   A^T y = BP_ref(y / L^2), with L the ray length in voxels, for rays that
-  are neither exactly diagonal nor short.
+  are neither exactly diagonal nor short;
+* the distance-driven FDK backprojection and the trilinear warp at the FDK
+  scanner's and the motion workload's sizes.
 """
 import numpy as np
 import pytest
@@ -99,3 +101,42 @@ def test_autograd_gradient_vs_reference_backprojector(cuda, oracle_lib):
     ref = ref_backproject(oracle_lib, og, yl, ang, (si, sd, na, px, 0.5, nbr, px, 0.5), atomic=False)
     r, m = rel(grad, ref)
     assert r <= 1e-5 and m <= 1e-4, (r, m)
+
+
+def test_distance_driven_full_size_vs_reference(cuda, oracle_lib):
+    """The distance-driven FDK backprojection at the FDK scanner's size
+    (256^3, 512 x 384 bins of 1.2 voxels, 600 / 1200 voxels), 8 views,
+    against the reference's dist_3d_back_fdk kernel built for the host."""
+    if not oracle_lib.have_ref():
+        pytest.skip("the reference's host build is absent")
+    n, na, nbr, px, sad, sid = 256, 512, 384, 1.2, 600.0, 1200.0
+    ang = (np.linspace(0, 2 * np.pi, 8, endpoint=False) + 0.3).astype(np.float32)
+    proj = torch.rand((8, nbr, na), device=cuda, generator=torch.Generator(device=cuda).manual_seed(5))
+    ours = ops.dd_backproject(proj, (n, n, n), ang, sad, sid, px, px).cpu().numpy()
+    ref = oracle_lib.ref_dd_backproject(proj.cpu().numpy(), ang, (n, n, n), sid, sad, na, px, 0.0, nbr, px, 0.0)
+    r, m = rel(ours, ref)
+    assert r <= 1e-5 and m <= 1e-4, (r, m)
+
+
+def test_warp_full_size_vs_reference(cuda, oracle_lib):
+    """The trilinear warp at the motion workload's size (256^3, a field of
+    four sinusoids per component up to 5 voxels) against the reference's
+    DeformKernel built for the host."""
+    if not oracle_lib.have_ref():
+        pytest.skip("the reference's host build is absent")
+    n = 256
+    gen = torch.Generator(device=cuda).manual_seed(5)
+    img = torch.rand((n, n, n), device=cuda, generator=gen)
+    z, y, x = torch.meshgrid(*[torch.arange(n, device=cuda, dtype=torch.float32)] * 3, indexing="ij")
+    rng = np.random.default_rng(5)
+    m = []
+    for _ in range(3):
+        f = torch.zeros_like(img)
+        for _ in range(4):
+            k, ph = rng.uniform(0.5, 3, 3) * 2 * np.pi / n, rng.uniform(0, 2 * np.pi)
+            f += 1.25 * torch.sin(float(k[0]) * x + float(k[1]) * y + float(k[2]) * z + float(ph))
+        m.append(f.contiguous())
+    ours = ops.warp_forward(img, *m).cpu().numpy()
+    ref = oracle_lib.ref_deform(img.cpu().numpy(), *[a.cpu().numpy() for a in m])
+    r, mx = rel(ours, ref)
+    assert r <= 1e-5 and mx <= 1e-4, (r, mx)

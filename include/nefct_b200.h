@@ -221,6 +221,16 @@ int64_t nefct_cb_batch_tiles(const nefct_cb_batch *plan);   /* work tiles per la
 #define NEFCT_BATCH_PERSISTENT  0
 #define NEFCT_BATCH_PER_PROBLEM 1
 nefct_status nefct_cb_batch_set_strategy(nefct_cb_batch *plan, int32_t strategy);
+/* Host-only: points the plan's problems at other buffers of the same shapes
+ * (arrays of n pointers in the caller's problem order; a NULL array or a
+ * NULL entry keeps the current buffer), so a caller can run the batch on
+ * tensors it already holds instead of copying them into the bound ones.
+ * Takes effect from the next forward / backward (their launches copy the
+ * pointers when they are issued); a CUDA graph keeps the pointers it was
+ * captured with.  The buffers must stay valid while the plan uses them.  No
+ * counterpart in the reference. */
+nefct_status nefct_cb_batch_set_buffers(nefct_cb_batch *plan, const float *const *vols, float *const *sinos,
+                                        const float *const *grads, float *const *backs);
 void nefct_cb_batch_destroy(nefct_cb_batch *plan);
 
 /* LOR projector pair.  lors is [6][n] (rows x1 y1 z1 x2 y2 z2, each n

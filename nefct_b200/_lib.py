@@ -97,6 +97,7 @@ _PROTOS = {
     "nefct_cb_batch_backward": (_i32, [_vp, _vp]),
     "nefct_cb_batch_tiles": (C.c_int64, [_vp]),
     "nefct_cb_batch_set_strategy": (_i32, [_vp, _i32]),
+    "nefct_cb_batch_set_buffers": (_i32, [_vp, _vp, _vp, _vp, _vp]),
     "nefct_cb_batch_destroy": (None, [_vp]),
     "nefct_lor_forward": (_i32, [C.POINTER(Grid), _vp, C.c_int64, _vp, _vp, _u32, _vp]),
     "nefct_lor_backward": (_i32, [C.POINTER(Grid), _vp, C.c_int64, _vp, _vp, _u32, _vp]),

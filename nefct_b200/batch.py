@@ -21,31 +21,57 @@ from . import _lib, ops
 __all__ = ["BatchProjector", "batch_project"]
 
 
+def _direct(t: torch.Tensor | None, like: torch.Tensor) -> bool:
+    """True when t can be read by the plan in place of its bound tensor."""
+    return (t is not None and t.is_contiguous() and t.dtype == torch.float32 and t.device == like.device
+            and t.shape == like.shape)
+
+
 class _BatchProject(torch.autograd.Function):
     """Forward: the plan's batched forward of every problem; backward: the
-    plan's batched exact transpose of the incoming gradients.  Volumes that
-    are not the plan's own bound tensors are copied into them first; the
-    returned sinograms are the plan's bound output tensors (no copy), valid
-    until the plan's next forward."""
+    plan's batched exact transpose of the incoming gradients.  Inputs are
+    read in place (the plan is pointed at them for the one launch, then back
+    at its own tensors) when they are contiguous float32 tensors of the
+    plan's shapes, else copied into the bound tensors; the returned sinograms
+    are the plan's bound output tensors (no copy), valid until the plan's
+    next forward."""
 
     @staticmethod
     def forward(ctx, bp, *vols):
-        for v, dst in zip(vols, bp.vols):
-            if v.data_ptr() != dst.data_ptr():
+        use = [v if _direct(v, dst) else None for v, dst in zip(vols, bp.vols)]
+        for v, u, dst in zip(vols, use, bp.vols):
+            if u is None and v.data_ptr() != dst.data_ptr():
                 dst.copy_(v)
-        bp.forward()
+        rebound = any(u is not None and u.data_ptr() != dst.data_ptr() for u, dst in zip(use, bp.vols))
+        if rebound:
+            bp._set_buffers(vols=use)
+        try:
+            bp.forward()
+        finally:
+            if rebound:
+                bp._set_buffers(vols=bp.vols)
         ctx.bp = bp
         return tuple(bp.sinos)
 
     @staticmethod
     def backward(ctx, *grads):
         bp = ctx.bp
-        for g, dst in zip(grads, bp.grads):
+        use = [g if _direct(g, dst) else None for g, dst in zip(grads, bp.grads)]
+        for g, u, dst in zip(grads, use, bp.grads):
+            if u is not None:
+                continue
             if g is None:
                 dst.zero_()
             elif g.data_ptr() != dst.data_ptr():
                 dst.copy_(g)
-        bp.backward()
+        rebound = any(u is not None and u.data_ptr() != dst.data_ptr() for u, dst in zip(use, bp.grads))
+        if rebound:
+            bp._set_buffers(grads=use)
+        try:
+            bp.backward()
+        finally:
+            if rebound:
+                bp._set_buffers(grads=bp.grads)
         return (None, *bp.backs)
 
 
@@ -163,6 +189,16 @@ class BatchProjector:
 
     def _stream(self):
         return torch.cuda.current_stream(self.device).cuda_stream
+
+    def _set_buffers(self, vols=None, grads=None):
+        """Points the plan's problems at other volumes / gradient sinograms
+        (lists in problem order; None entries keep the current buffer) until
+        the next call (nefct_cb_batch_set_buffers; host-only)."""
+        def arr(ts):
+            if ts is None:
+                return None
+            return (C.c_void_p * len(ts))(*[None if t is None else t.data_ptr() for t in ts])
+        _lib.check(_lib.load().nefct_cb_batch_set_buffers(self._plan, arr(vols), None, arr(grads), None))
 
     def forward(self):
         _lib.check(_lib.load().nefct_cb_batch_forward(self._plan, self._stream()))

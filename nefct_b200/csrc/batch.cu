@@ -498,6 +498,28 @@ nefct_status nefct_cb_batch_set_strategy(nefct_cb_batch *b, int32_t strategy)
     return NEFCT_OK;
 }
 
+nefct_status nefct_cb_batch_set_buffers(nefct_cb_batch *b, const float *const *vols, float *const *sinos,
+                                        const float *const *grads, float *const *backs)
+{
+    if (!b) return fail(NEFCT_ERR_INVALID, "plan is NULL");
+    const int n = (int)b->desc.size();
+    for (int k = 0; k < n; ++k) {
+        const int i = b->order[k];
+        nefct_cb_problem &P = b->probs[i];
+        if (vols && vols[i]) P.vol = vols[i];
+        if (sinos && sinos[i]) P.sino = sinos[i];
+        if (grads && grads[i]) P.grad = grads[i];
+        if (backs && backs[i]) P.back = backs[i];
+        BatchDesc &D = b->desc[k];
+        D.vol = P.vol; D.sino = P.sino; D.grad = P.grad; D.back = P.back;
+        if (b->args) {
+            BatchDesc &A = b->args->d[k];
+            A.vol = P.vol; A.sino = P.sino; A.grad = P.grad; A.back = P.back;
+        }
+    }
+    return NEFCT_OK;
+}
+
 void nefct_cb_batch_destroy(nefct_cb_batch *b) { delete b; }
 
 }  // extern "C"

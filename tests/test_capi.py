@@ -121,6 +121,25 @@ def test_batch_plan_validates_problems(nefct_lib):
     assert nefct_lib.nefct_cb_batch_plan(probs, 1, 0x4000, C.byref(plan), C.byref(ws)) == 1  # unknown flags
 
 
+def test_batch_set_buffers_is_host_only(nefct_lib):
+    """Planning and re-pointing a plan's buffers make no CUDA call (fake
+    device pointers are only stored); a NULL plan is refused."""
+    from nefct_b200 import _lib
+    probs = (_lib.CBProblem * 2)()
+    for i in range(2):
+        probs[i].geom = _geom().struct()
+        probs[i].vol = probs[i].sino = probs[i].grad = probs[i].back = 256 * (i + 1)
+    plan, ws = C.c_void_p(), C.c_size_t()
+    assert nefct_lib.nefct_cb_batch_plan(probs, 2, 0, C.byref(plan), C.byref(ws)) == 0
+    try:
+        vols = (C.c_void_p * 2)(4096, None)
+        assert nefct_lib.nefct_cb_batch_set_buffers(plan, vols, None, None, None) == 0
+        assert nefct_lib.nefct_cb_batch_set_buffers(plan, None, None, vols, None) == 0
+    finally:
+        nefct_lib.nefct_cb_batch_destroy(plan)
+    assert nefct_lib.nefct_cb_batch_set_buffers(None, None, None, None, None) == 1
+
+
 def test_dd_rejects_bad_geometry(nefct_lib):
     from nefct_b200 import _lib
     ang = (C.c_float * 2)(0.0, float("nan"))

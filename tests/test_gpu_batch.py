@@ -124,23 +124,32 @@ def test_batch_vs_reference_build(cuda, oracle_lib, strategy):
                     assert_parity(b.cpu().numpy(), rb)
 
 
-def test_batch_autograd_function(cuda):
+@pytest.mark.parametrize("strategy", ["persistent", "per-problem"])
+def test_batch_autograd_function(cuda, strategy):
     """batch_project: the batched forward as a torch.autograd.Function; the
     gradient of sum_i ||A_i x_i - b_i||^2 / 2 comes from one batched
-    transpose and matches per-problem autograd through nb.project."""
+    transpose and matches per-problem autograd through nb.project.  The
+    inputs and incoming gradients are read in place (the plan is pointed at
+    them for the launch), and the plan is pointed back at its own tensors
+    afterwards."""
     from nefct_b200.batch import batch_project
     geoms, vols, _ = _problems(cuda)
     targets = [ops.cb_forward(v * 0.5, g) for g, v in zip(geoms, vols)]
     xs = [v.clone().requires_grad_() for v in vols]
-    bp = BatchProjector(geoms, [v.detach().clone() for v in vols], grads=[torch.empty_like(t) for t in targets],
-                        strategy="persistent")
+    own = [torch.rand_like(v) for v in vols]
+    bp = BatchProjector(geoms, own, grads=[torch.empty_like(t) for t in targets], strategy=strategy)
     sinos = batch_project(bp, xs)
+    for g, x, s_ in zip(geoms, xs, sinos):
+        assert torch.equal(s_, ops.cb_forward(x.detach(), g))
     loss = sum(((s - t) ** 2).sum() / 2 for s, t in zip(sinos, targets))
     loss.backward()
     for g, x, t in zip(geoms, xs, targets):
         xr = x.detach().clone().requires_grad_()
         (((nb.project(xr, g) - t) ** 2).sum() / 2).backward()
         assert_parity(x.grad.cpu().numpy(), xr.grad.cpu().numpy())
+    bp.forward()                                  # back on the plan's own volumes
+    for g, v, s_ in zip(geoms, own, bp.sinos):
+        assert torch.equal(s_, ops.cb_forward(v, g))
 
 
 def test_batch_tile_shape_autotuning(cuda):

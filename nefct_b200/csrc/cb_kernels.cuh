@@ -138,7 +138,7 @@ __device__ __forceinline__ void colwarp_lane(const GridDev<float> &g, const floa
 #pragma unroll
             for (int i = 0; i < s.n; ++i) acc += v[i] * s.r[i];
         };
-        col_walk_any<DIV, false>(c, L, K0, K1, KI0, KI1, g, f);
+        col_walk_any<DIV, 0>(c, L, K0, K1, KI0, KI1, g, f);
         if (has) *out = live ? acc * w.W : 0.f;
     } else if constexpr (FIX) {
         const float yw = y * w.W;
@@ -147,15 +147,21 @@ __device__ __forceinline__ void colwarp_lane(const GridDev<float> &g, const floa
             for (int i = 0; i < s.n; ++i)
                 if (s.ok[i]) atomicAdd(fixZ + s.idx[i], (unsigned long long)to_fixed((yw * s.r[i]) * scale));
         };
-        col_walk_any<DIV, true>(c, L, K0, K1, KI0, KI1, g, f);
+        col_walk_any<DIV, 1>(c, L, K0, K1, KI0, KI1, g, f);
     } else {
         const float yw = y * w.W;
         auto f = [&](const auto &s) {
+            if constexpr (s.n == 2) {
+                // the two-slot split's weights are r and 1 - r: y w (1 - r) in one rounding
+                if (s.ok[0]) atomicAdd(accZ + s.idx[0], yw * s.r[0]);
+                if (s.ok[1]) atomicAdd(accZ + s.idx[1], fmaf(-yw, s.r[0], yw));
+            } else {
 #pragma unroll
-            for (int i = 0; i < s.n; ++i)
-                if (s.ok[i]) atomicAdd(accZ + s.idx[i], yw * s.r[i]);
+                for (int i = 0; i < s.n; ++i)
+                    if (s.ok[i]) atomicAdd(accZ + s.idx[i], yw * s.r[i]);
+            }
         };
-        col_walk_any<DIV, true>(c, L, K0, K1, KI0, KI1, g, f);
+        col_walk_any<DIV, 2>(c, L, K0, K1, KI0, KI1, g, f);
     }
 }
 

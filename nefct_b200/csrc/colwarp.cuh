@@ -109,10 +109,14 @@ template <int NS, bool CHK> struct ColSlots {
 // by the warp (b1 != b2): without one (VX false) the split has two slots,
 // (v1, w1) with ratio rw and (v1, w2) with 1 - rw, which is the general
 // three-slot split with rv = 1 (its third ratio, 1 - max(rv, rw), is 0 and
-// its slot inactive); with one, the general split.  SPLIT false takes the
+// its slot inactive); with one, the general split.  SPLIT 0 takes the
 // general split for every slab (no branch: the forward's loads of
-// consecutive slabs interleave better).  f(slots) consumes.
-template <bool DIV, bool CHECK, int WUP, bool SPLIT, class Fn>
+// consecutive slabs interleave better); 1 the two-slot split; 2 the same
+// with the second slot always at w2 (it differs from the reference's pairing
+// only when the ratio rounds to 1 or above, where that slot's weight is a
+// rounding error; for the float transpose, whose atomic sums are not
+// reproducible anyway).  f(slots) consumes.
+template <bool DIV, bool CHECK, int WUP, int SPLIT, class Fn>
 __device__ __forceinline__ void col_slab(ColLane &L, float dz, bool zdiv, float nz2, int nv, int nz,
                                          const ColTable &tab, int j, Fn &f)
 {
@@ -143,7 +147,7 @@ __device__ __forceinline__ void col_slab(ColLane &L, float dz, bool zdiv, float 
         s.r[0] = rw;                            // min(1, rw)
         s.r[1] = __fsub_rn(1.f, rw);            // |1 - rw|
         s.idx[0] = b1 + i1;
-        s.idx[1] = b1 + (vfirst ? i2 : i1);
+        s.idx[1] = b1 + ((SPLIT == 2 || vfirst) ? i2 : i1);
         if (CHECK) {
             const bool adm = L.live && (unsigned)cv1 < (unsigned)nv && (unsigned)(cw1 + (int)wx) < (unsigned)(nz + (int)wx);
             const int mw = vfirst ? cw2 : cw1;
@@ -184,7 +188,7 @@ __device__ __forceinline__ void col_slab(ColLane &L, float dz, bool zdiv, float 
 
 // Walks slabs [a, b] (inside the current 32-slab chunk starting at kc) in
 // one check mode.
-template <bool DIV, bool CHECK, int WUP, bool SPLIT, class Fn>
+template <bool DIV, bool CHECK, int WUP, int SPLIT, class Fn>
 __device__ __forceinline__ void col_range(int a, int b, int kc, const ColShared &c, ColLane &L,
                                           const ColTable &tab, const GridDev<float> &g, Fn &f)
 {
@@ -199,7 +203,7 @@ __device__ __forceinline__ void col_range(int a, int b, int kc, const ColShared 
 // range checks.  The slab planes k - nu2 and k + 1 - nu2 are exact (nu2 is a
 // multiple of 1/2 and |k| < 2^22), so the table's exit plane offset equals
 // the one a walk carrying t += 1 evaluates.
-template <bool DIV, int WUP, bool SPLIT, class Fn>
+template <bool DIV, int WUP, int SPLIT, class Fn>
 __device__ __forceinline__ void col_walk(const ColShared &c, ColLane &L, int K0, int K1, int KI0, int KI1,
                                          const GridDev<float> &g, ColTable &tab, Fn &f)
 {
@@ -225,7 +229,7 @@ __device__ __forceinline__ void col_walk(const ColShared &c, ColLane &L, int K0,
     }
 }
 
-template <bool DIV, bool SPLIT, class Fn>
+template <bool DIV, int SPLIT, class Fn>
 __device__ __forceinline__ void col_walk_any(const ColShared &c, ColLane &L, int K0, int K1, int KI0, int KI1,
                                              const GridDev<float> &g, Fn &f)
 {

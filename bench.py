@@ -88,6 +88,16 @@ def load_traffic(workload):
     return {}
 
 
+def load_issue(workload):
+    """Warp instructions per view of each kernel of a workload, from the
+    committed ncu summary (profiles/issue.json)."""
+    p = os.path.join(ROOT, "profiles", "issue.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f).get(workload, {})
+    return {}
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -432,6 +442,10 @@ def run_gpu(args):
     names = {"fwd": "cb_colwarp_kernel<forward>" if walk & 1 else "cb_forward_kernel",
              "bwd": "cb_colwarp_kernel<transpose>" if walk & 2 else "cb_backward_kernel"}
     traffic = load_traffic(args.workload)
+    issue = load_issue(args.workload)
+    clk_sum = clk.summary()
+    sm_hz = 1e6 * (clk_sum.get("sm_mhz") or clk_sum.get("sm_max_mhz") or 1965.0)
+    n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
     roof = {}
     for d, t, alg, comp in (("fwd", fwd_s, 4 * inter + 4 * rays, vbytes + sbytes),
                             ("bwd", bwd_s, 8 * inter + 4 * rays, 2 * vbytes + sbytes)):
@@ -444,6 +458,13 @@ def run_gpu(args):
                    "binding": "l2_read" if d == "fwd" and t_l2 >= t_hbm else
                               "l2_reductions" if t_l2 >= t_hbm else "hbm",
                    "frac_binding": max(t_hbm, t_l2) / t}
+        per_view = issue.get(names[d])
+        if per_view:
+            # one warp instruction per cycle on each of the 4 schedulers of every SM
+            inst = per_view * geom.nv
+            t_issue = inst / (4 * n_sm * sm_hz)
+            roof[d]["issue_ceiling"] = {"warp_instructions": inst, "ms": 1e3 * t_issue, "frac": t_issue / t,
+                                        "sm_mhz": sm_hz / 1e6}
     dom = "bwd" if bwd_s >= fwd_s else "fwd"
     rd = roof[dom]
     achieved = rd["algorithmic_bytes"] / (rd["ms"] / 1e3) / 1e9

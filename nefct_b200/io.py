@@ -5,8 +5,8 @@ Mirrors nefct/io/local_io_mixin.py:14-61 (``save`` / ``load`` and the
 nefct/io/json_io_mixin.py:17-70 (``json_dump(s)`` / ``json_load(s)``).
 
 The reference writes ``obj.asdict(recurse=True)`` with deepdish to HDF5.
-Neither deepdish nor h5py (nor an HDF5 library) is part of this build's
-environment, so ``save`` keeps the same dict tree in a numpy ``.npz``
+Neither deepdish nor h5py (nor an HDF5 library) is a dependency of this
+package, so ``save`` keeps the same dict tree in a numpy ``.npz``
 archive: every array of the tree is one entry (its key the path of names
 joined by '/'), and the rest of the tree (scalars, strings, lists, None,
 nesting) is one JSON entry, ``__tree__``, in which arrays appear as

@@ -15,8 +15,8 @@ Two layers:
   pin the restatement and as the "reference" CPU baseline.  Present only when
   it was built (it needs the reference checkout at build time).
 * ``_ref/libnefct_ref_gpu.so`` -- the reference's siddon_3d flat-detector
-  pair, pixel_3d backprojection and cpp/siddon LOR pair with their host
-  launchers, compiled by nvcc for the GPU (``ref_gpu_shim.cu``): the
+  pair, pixel_3d backprojection, cpp/siddon LOR pair and distance-driven FDK
+  backprojection with their host launchers, compiled by nvcc for the GPU (``ref_gpu_shim.cu``): the
   reference's own CUDA path, run on device buffers for parity and for timing
   beside the library.
 * ``_ref/libnefct_ref_tex.so`` -- the reference's texture-based DVF inversion
@@ -103,6 +103,10 @@ def _ref_gpu_lib():
             fn = getattr(_ref_gpu, name)
             fn.restype = C.c_int
             fn.argtypes = args
+        _ref_gpu.ref_gpu_dd_backproject_flat.restype = C.c_int
+        _ref_gpu.ref_gpu_dd_backproject_flat.argtypes = ([C.c_void_p] + [C.c_int] * 3 + [C.c_void_p] * 2
+                                                         + [C.c_int] + [C.c_float] * 4 + [C.c_int]
+                                                         + [C.c_float] * 2 + [C.c_int] + [C.c_void_p])
         lor_args = [C.c_void_p] + [C.c_int] * 4 + [C.c_float] * 6 + [C.c_void_p] * 2
         for name in ("ref_gpu_lor_forward", "ref_gpu_lor_backward"):
             fn = getattr(_ref_gpu, name)
@@ -130,6 +134,25 @@ def ref_gpu_pixel_backproject(sino, shape, corner, size, angles, SID, SAD, na, d
                                                   angles.contiguous().data_ptr(), na, nb, int(angles.numel()),
                                                   SID, SAD, da, ai, db, bi, out.data_ptr()),
                "pixel_3d backprojection")
+    return out
+
+
+def ref_gpu_dd_backproject(proj, shape, angles, offsets, SID, SAD, na, da, ai, nb, db, bi):
+    """The reference's distance-driven back_project_fdk_kernel through
+    back_project_flat_fdk_gpu (dist_3d_back_fdk.cu.cc:17-276) on the GPU, in
+    its naming (SID source-detector, SAD source-axis, voxel units).  proj:
+    float32 CUDA tensor [nv][nb][na]; angles, offsets: float32 CUDA tensors
+    [nv]; returns the volume [nz][ny][nx] (zeroed, then added into).
+    Synchronises."""
+    import torch
+    lib_ = _ref_gpu_lib()
+    assert proj.is_cuda and proj.dtype == torch.float32 and proj.is_contiguous()
+    nx, ny, nz = shape
+    out = torch.zeros((nz, ny, nx), dtype=torch.float32, device=proj.device)
+    _check_gpu(lib_.ref_gpu_dd_backproject_flat(proj.data_ptr(), nx, ny, nz, offsets.contiguous().data_ptr(),
+                                                angles.contiguous().data_ptr(), int(angles.numel()), SID, SAD,
+                                                da, ai, na, db, bi, nb, out.data_ptr()),
+               "distance-driven backprojection")
     return out
 
 

@@ -5,6 +5,8 @@
 //   pixel3d_gpu.inc   nefct/cc/pixel_3d/pixel.cu.cc:6-204 (voxel-driven
 //                     backprojection)
 //   lor_gpu.inc       cpp/siddon/siddon_gpu.cu.cc:6-747 (LOR pair)
+//   dd_fdk_gpu.inc    nefct/cc/distance_3d/dist_3d_back_fdk.cu.cc:6-298
+//                     (distance-driven FDK backprojection)
 // Each file sits in its own namespace (they share function names).  It runs
 // the reference's own CUDA path on the GPU for the parity tests and for
 // timing that path beside the library's.  Only tests load it.
@@ -16,7 +18,10 @@
 // ia + ib*na + iv*na*nb and the LOR index tid < num_events stay in their
 // buffers.  The cylindrical siddon_3d backprojection reads its sinogram at
 // ia + iv*na + ib*na*nb (quirk Q8, siddon.cu.cc:830), which leaves the
-// buffer when nb > nv, so only the flat variants are exported.
+// buffer when nb > nv, so only the flat variants are exported.  The
+// distance-driven kernel adds into voxels ix < nx, max(0, Yi1) <= iy <=
+// min(ny - 1, Yi2), max(0, Zi1) <= iz <= min(nz - 1, Zi2) and reads its bin
+// id < na*nb*nv.
 #include <cuda_runtime.h>
 #include <stddef.h>
 
@@ -32,6 +37,14 @@ namespace lor {
 #include "lor_gpu.inc"
 }
 #undef abs
+namespace ddf {
+#include "dd_fdk_gpu.inc"
+}
+#undef ABS
+#undef MAX
+#undef MIN
+#undef MAX4
+#undef MIN4
 
 namespace {
 
@@ -118,6 +131,20 @@ int ref_gpu_lor_backward(const float *lors, int n, int nx, int ny, int nz, float
     return with_grid({{nx, ny, nz}, {cx, cy, cz}, {sx, sy, sz}}, [&](const int *g, const float *c, const float *s) {
         lor::backprojection(lors, lors + r, lors + 2 * r, lors + 3 * r, lors + 4 * r, lors + 5 * r, vals, g, c, s, vol,
                             n);
+    });
+}
+
+// dist_3d_back_fdk.cu.cc:257-276 (flat detector), the reference's naming
+// (SID source-detector, SAD source-axis, voxel units): proj device
+// [nv][nb][na], offsets / angles device [nv]; adds into vol [nz][ny][nx]
+// (zero it first).
+int ref_gpu_dd_backproject_flat(const float *proj, int nx, int ny, int nz, const float *offsets, const float *angles,
+                                int nv, float SID, float SAD, float da, float ai, int na, float db, float bi, int nb,
+                                float *vol)
+{
+    const HostGrid hg = {{nx, ny, nz}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+    return with_grid(hg, [&](const int *g, const float *, const float *) {
+        ddf::back_project_flat_fdk_gpu(proj, g, offsets, angles, nv, SID, SAD, da, ai, na, db, bi, nb, vol);
     });
 }
 

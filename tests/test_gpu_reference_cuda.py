@@ -1,14 +1,15 @@
 """GPU: the library against the reference's own CUDA kernels, built
 unchanged by nvcc from the reference sources (oracle/_ref/libnefct_ref_gpu.so:
 siddon_3d's ProjectFlatKernel / BackProjectFlatKernel, pixel_3d's
-BackProjectFlatKernel and cpp/siddon's ProjectKernel / BackProjectKernel with
-their host launchers) and run on the same GPU.
+BackProjectFlatKernel, cpp/siddon's ProjectKernel / BackProjectKernel and
+dist_3d_back_fdk's back_project_fdk_kernel with their host launchers) and run
+on the same GPU.
 
 * parity: the library's outputs against the reference's CUDA kernels,
   element-wise (rel-L2 <= 1e-5, max-abs <= 1e-4 x max): the cone-beam pair on
   the 64^3 workload at full size and on views of the 512^3 scan, the
-  voxel-driven backprojection on the FDK scanner, the LOR pair on 4 Mi ring
-  lines;
+  voxel-driven and the distance-driven backprojections on the FDK scanner,
+  the LOR pair on 1 Mi ring lines;
 * speed: each reference launch beside the library's call for the same work,
   both timed with CUDA events after a warm-up call, the fastest of three
   (printed with -s).
@@ -181,3 +182,23 @@ def test_reference_cuda_lor_pair(cuda, oracle_lib):
           f"{t_ref_b:.1f} ms; library (ordered walk) forward {t_f:.2f} ms, backprojection {t_b:.2f} ms "
           f"({t_ref_f / t_f:.1f}x, {t_ref_b / t_b:.1f}x)")
     assert t_f < t_ref_f and t_b < t_ref_b
+
+
+def test_reference_cuda_distance_driven_backprojection(cuda, oracle_lib):
+    """The distance-driven FDK backprojection (dist_3d_back_fdk.cu.cc) on 72
+    views of the FDK scanner in voxel units (256^3, 512 x 384 bins of 1.2,
+    source-axis 600, source-detector 1200), against the reference's CUDA
+    kernel (a thread per bin, atomics into the x-fastest volume)."""
+    n, nv, na, nbr, px, sad, sid = 256, 72, 512, 384, 1.2, 600.0, 1200.0
+    ang = (np.linspace(0, 2 * np.pi, nv, endpoint=False)).astype(np.float32)
+    proj = torch.rand((nv, nbr, na), device=cuda, generator=torch.Generator(device=cuda).manual_seed(21))
+    d_ang = torch.from_numpy(ang).to(cuda)
+    d_off = torch.zeros(nv, device=cuda)
+    ref, t_ref = _events(lambda: oracle_lib.ref_gpu_dd_backproject(proj, (n, n, n), d_ang, d_off, sid, sad, na, px,
+                                                                    0.0, nbr, px, 0.0))
+    out, t = _events(lambda: ops.dd_backproject(proj, (n, n, n), ang, sad, sid, px, px))
+    r, m = rel(out, ref)
+    assert r <= 1e-5 and m <= 1e-4, (r, m)
+    print(f"\ndistance-driven backprojection, 256^3 x 72 views: reference CUDA {t_ref:.1f} ms, library {t:.2f} ms "
+          f"({t_ref / t:.1f}x)")
+    assert t < t_ref

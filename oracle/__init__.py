@@ -15,8 +15,8 @@ Two layers:
   pin the restatement and as the "reference" CPU baseline.  Present only when
   it was built (it needs the reference checkout at build time).
 * ``_ref/libnefct_ref_gpu.so`` -- the reference's siddon_3d flat-detector
-  pair, pixel_3d backprojection, cpp/siddon LOR pair and distance-driven FDK
-  backprojection with their host launchers, compiled by nvcc for the GPU (``ref_gpu_shim.cu``): the
+  pair, pixel_3d backprojection, cpp/siddon LOR pair, distance-driven FDK
+  backprojection and cpp/deform warp with their host launchers, compiled by nvcc for the GPU (``ref_gpu_shim.cu``): the
   reference's own CUDA path, run on device buffers for parity and for timing
   beside the library.
 * ``_ref/libnefct_ref_tex.so`` -- the reference's texture-based DVF inversion
@@ -107,6 +107,8 @@ def _ref_gpu_lib():
         _ref_gpu.ref_gpu_dd_backproject_flat.argtypes = ([C.c_void_p] + [C.c_int] * 3 + [C.c_void_p] * 2
                                                          + [C.c_int] + [C.c_float] * 4 + [C.c_int]
                                                          + [C.c_float] * 2 + [C.c_int] + [C.c_void_p])
+        _ref_gpu.ref_gpu_deform.restype = C.c_int
+        _ref_gpu.ref_gpu_deform.argtypes = [C.c_void_p] * 4 + [C.c_int] * 3 + [C.c_void_p]
         lor_args = [C.c_void_p] + [C.c_int] * 4 + [C.c_float] * 6 + [C.c_void_p] * 2
         for name in ("ref_gpu_lor_forward", "ref_gpu_lor_backward"):
             fn = getattr(_ref_gpu, name)
@@ -153,6 +155,22 @@ def ref_gpu_dd_backproject(proj, shape, angles, offsets, SID, SAD, na, da, ai, n
                                                 angles.contiguous().data_ptr(), int(angles.numel()), SID, SAD,
                                                 da, ai, na, db, bi, nb, out.data_ptr()),
                "distance-driven backprojection")
+    return out
+
+
+def ref_gpu_deform(img, mx, my, mz):
+    """The reference's cpp/deform DeformKernel through deform()
+    (deform.cu.cc:14-46, 112-126) on the GPU: float32 CUDA tensors
+    [nz][ny][nx]; returns the warped image (zero where the reference writes
+    nothing, Q13).  Synchronises."""
+    import torch
+    lib_ = _ref_gpu_lib()
+    ts = [t.contiguous() for t in (img, mx, my, mz)]
+    for t in ts:
+        assert t.is_cuda and t.dtype == torch.float32 and t.shape == ts[0].shape
+    nz, ny, nx = ts[0].shape
+    out = torch.zeros_like(ts[0])
+    _check_gpu(lib_.ref_gpu_deform(*[t.data_ptr() for t in ts], nx, ny, nz, out.data_ptr()), "deform")
     return out
 
 

@@ -7,6 +7,7 @@
 //   lor_gpu.inc       cpp/siddon/siddon_gpu.cu.cc:6-747 (LOR pair)
 //   dd_fdk_gpu.inc    nefct/cc/distance_3d/dist_3d_back_fdk.cu.cc:6-298
 //                     (distance-driven FDK backprojection)
+//   deform_gpu.inc    cpp/deform/deform.cu.cc:6-126 (trilinear warp)
 // Each file sits in its own namespace (they share function names).  It runs
 // the reference's own CUDA path on the GPU for the parity tests and for
 // timing that path beside the library's.  Only tests load it.
@@ -21,7 +22,8 @@
 // buffer when nb > nv, so only the flat variants are exported.  The
 // distance-driven kernel adds into voxels ix < nx, max(0, Yi1) <= iy <=
 // min(ny - 1, Yi2), max(0, Zi1) <= iz <= min(nz - 1, Zi2) and reads its bin
-// id < na*nb*nv.
+// id < na*nb*nv; the warp reads its 8 taps only when 0 < xi, xi + 1 < nx
+// (and the same in y, z).
 #include <cuda_runtime.h>
 #include <stddef.h>
 
@@ -45,6 +47,10 @@ namespace ddf {
 #undef MIN
 #undef MAX4
 #undef MIN4
+namespace dfm {
+#include "deform_gpu.inc"
+}
+#undef abs
 
 namespace {
 
@@ -146,6 +152,16 @@ int ref_gpu_dd_backproject_flat(const float *proj, int nx, int ny, int nz, const
     return with_grid(hg, [&](const int *g, const float *, const float *) {
         ddf::back_project_flat_fdk_gpu(proj, g, offsets, angles, nv, SID, SAD, da, ai, na, db, bi, nb, vol);
     });
+}
+
+// cpp/deform deform (deform.cu.cc:112-126): img, mx, my, mz, out device
+// [nz][ny][nx]; out is written where the reference writes (Q13: zero it
+// first).
+int ref_gpu_deform(const float *img, const float *mx, const float *my, const float *mz, int nx, int ny, int nz,
+                   float *out)
+{
+    const HostGrid hg = {{nx, ny, nz}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+    return with_grid(hg, [&](const int *g, const float *, const float *) { dfm::deform(img, mx, my, mz, g, out); });
 }
 
 }  // extern "C"

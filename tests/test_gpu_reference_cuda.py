@@ -2,14 +2,14 @@
 unchanged by nvcc from the reference sources (oracle/_ref/libnefct_ref_gpu.so:
 siddon_3d's ProjectFlatKernel / BackProjectFlatKernel, pixel_3d's
 BackProjectFlatKernel, cpp/siddon's ProjectKernel / BackProjectKernel and
-dist_3d_back_fdk's back_project_fdk_kernel with their host launchers) and run
-on the same GPU.
+dist_3d_back_fdk's back_project_fdk_kernel and cpp/deform's DeformKernel
+with their host launchers) and run on the same GPU.
 
 * parity: the library's outputs against the reference's CUDA kernels,
   element-wise (rel-L2 <= 1e-5, max-abs <= 1e-4 x max): the cone-beam pair on
   the 64^3 workload at full size and on views of the 512^3 scan, the
   voxel-driven and the distance-driven backprojections on the FDK scanner,
-  the LOR pair on 1 Mi ring lines;
+  the LOR pair on 1 Mi ring lines, the warp at 256^3;
 * speed: each reference launch beside the library's call for the same work,
   both timed with CUDA events after a warm-up call, the fastest of three
   (printed with -s).
@@ -202,3 +202,26 @@ def test_reference_cuda_distance_driven_backprojection(cuda, oracle_lib):
     print(f"\ndistance-driven backprojection, 256^3 x 72 views: reference CUDA {t_ref:.1f} ms, library {t:.2f} ms "
           f"({t_ref / t:.1f}x)")
     assert t < t_ref
+
+
+def test_reference_cuda_warp(cuda, oracle_lib):
+    """The trilinear warp at the motion workload's size (256^3, a field of
+    four sinusoids per component up to 5 voxels) against the reference's
+    cpp/deform CUDA kernel."""
+    n = 256
+    gen = torch.Generator(device=cuda).manual_seed(6)
+    img = torch.rand((n, n, n), device=cuda, generator=gen)
+    z, y, x = torch.meshgrid(*[torch.arange(n, device=cuda, dtype=torch.float32)] * 3, indexing="ij")
+    rng = np.random.default_rng(6)
+    m = []
+    for _ in range(3):
+        f = torch.zeros_like(img)
+        for _ in range(4):
+            k, ph = rng.uniform(0.5, 3, 3) * 2 * np.pi / n, rng.uniform(0, 2 * np.pi)
+            f += 1.25 * torch.sin(float(k[0]) * x + float(k[1]) * y + float(k[2]) * z + float(ph))
+        m.append(f.contiguous())
+    ref, t_ref = _events(lambda: oracle_lib.ref_gpu_deform(img, *m))
+    out, t = _events(lambda: ops.warp_forward(img, *m))
+    r, mx = rel(out, ref)
+    assert r <= 1e-5 and mx <= 1e-4, (r, mx)
+    print(f"\ntrilinear warp, 256^3: reference CUDA {t_ref:.3f} ms, library {t:.3f} ms ({t_ref / t:.1f}x)")

@@ -149,12 +149,14 @@ def dist_setup():
     import torch
     import torch.distributed as dist
     ws = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0")) if ws > 1 else 0
+    torch.cuda.set_device(local)                     # before the group: its communicator binds this GPU
     if ws > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-        rank, local = dist.get_rank(), int(os.environ.get("LOCAL_RANK", "0"))
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        rank = dist.get_rank()
     else:
-        rank, local = 0, 0
-    torch.cuda.set_device(local)
+        rank = 0
     return rank, ws, local
 
 

@@ -553,9 +553,28 @@ __global__ void __launch_bounds__(128) fdk_bp_kernel(const __grid_constant__ BpP
         float r0, r1, wb, wb2;
         if (fabsf(c.bm) * zabs + fabsf(p.cb) < 2097152.f) {
 #pragma unroll
-            for (int k = 0; k < kZ; ++k)
-                if (bp_tap<QUAD>(p, pv, pq, c, __fmaf_rn(c.bm, zc[k], p.cb), r0, r1, wb, wb2))
-                    acc[k] = __fmaf_rn(r1, wb2, __fmaf_rn(r0, wb, acc[k]));
+            for (int k = 0; k < kZ; ++k) {
+                // branch-free: a dropped row (Q11) reads row nb - 2's taps with
+                // zero weights (adds +0: measured 2.6 % faster than skipping)
+                const float b = __fmaf_rn(c.bm, zc[k], p.cb);
+                const float mb = __fadd_rd(b, 12582912.0f);
+                const unsigned ib = (unsigned)(__float_as_int(mb) - 0x4B400000);
+                const bool keep = ib < (unsigned)(p.nb - 1);
+                const unsigned ibc = keep ? ib : (unsigned)(p.nb - 2);
+                const float w2 = __fsub_rn(b, __fsub_rn(mb, 12582912.0f));
+                const float wb2k = keep ? w2 : 0.f, wbk = keep ? __fsub_rn(1.f, w2) : 0.f;
+                float t00, t01, t10, t11;
+                if (QUAD) {
+                    const float4 q4 = __ldg(pq + (size_t)ibc * p.na);
+                    t00 = q4.x; t01 = q4.y; t10 = q4.z; t11 = q4.w;
+                } else {
+                    const float *q = pv + (size_t)ibc * p.na;
+                    t00 = __ldg(q); t01 = __ldg(q + 1); t10 = __ldg(q + p.na); t11 = __ldg(q + p.na + 1);
+                }
+                const float a0 = __fmaf_rn(t01, c.wa2u, __fmul_rn(t00, c.wau));
+                const float a1 = __fmaf_rn(t11, c.wa2u, __fmul_rn(t10, c.wau));
+                acc[k] = __fmaf_rn(a1, wb2k, __fmaf_rn(a0, wbk, acc[k]));
+            }
         } else {
 #pragma unroll
             for (int k = 0; k < kZ; ++k)

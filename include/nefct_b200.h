@@ -284,8 +284,9 @@ nefct_status nefct_fdk_filter(const nefct_cb_geom *g, const float *sino, float *
  * low corner, Q10) times the FDK weight (src_iso / (src_iso + x'))^2 of
  * mat_codes/backprojection.m:12.  NEFCT_FDK_NO_WEIGHT drops the weight,
  * reproducing BackProjectFlat/BackProjectCyli of pixel_3d/pixel.cc:11-47.
- * A voxel whose detector column or row lies within 1/64 cell of the flat
- * detector's first or last (where Q11 keeps or drops it on a rounding) is
+ * A voxel whose detector column or row lies within a few thousandths of a
+ * cell of the flat detector's first or last (where Q11 keeps or drops it on
+ * a rounding) is
  * decided with the reference's own operations, so the same voxels are kept;
  * elsewhere the weights differ from the reference's by a few ulp. */
 #define NEFCT_FDK_NO_WEIGHT 0x100u

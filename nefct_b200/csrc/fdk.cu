@@ -652,7 +652,12 @@ __global__ void __launch_bounds__(256) fdk_edge_kernel(const __grid_constant__ B
     const float xc = bp_centre(ix, p.sx, p.nx, p.corner_x);
     const float yc = bp_centre(iy, p.sy, p.ny, p.corner_y);
     const float naf = (float)p.na, nbf = (float)p.nb;
-    const float edge = 1.f / 64 + fmaxf(naf, nbf) * (1.f / 16384);   // >> the few-ulp differences
+    // Width of the bands decided again: the kernel's detector coordinate
+    // differs from the reference's by a few ulp of terms of about half the
+    // detector (rcp_approx and the fused row: <= ~8 ulp of max(na, nb), i.e.
+    // under max(na, nb) * 2^-20); the band is 16x that plus 1/1024.  A
+    // wider band only adds work (every voxel in it is decided twice).
+    const float edge = 1.f / 1024 + fmaxf(naf, nbf) * (1.f / 65536);
     const size_t plane = (size_t)p.nx * p.ny;
     float *const vcol = vol + (size_t)iy * p.nx + ix;
     const float idz = (float)p.nz / p.sz;
@@ -703,14 +708,15 @@ __global__ void __launch_bounds__(256) fdk_edge_kernel(const __grid_constant__ B
         // voxel range of the band of rows within `edge` of row 0 (e = 0) or
         // nb - 1 (e = 1): the rows are monotone in z (b = bm z + cb), so the
         // band is one z interval, mapped to voxel indices in float with a
-        // margin of 1/64 voxel (its rounding is ~1e-4 voxel); the band is
-        // ~0.1 voxel wide, so most (column, view) pairs have no candidate
+        // margin of 1/1024 voxel (its rounding is ~1e-5 voxel); the band is
+        // a few thousandths of a voxel wide, so few (column, view) pairs have
+        // a candidate and few warps take the (divergent) candidate path
         float b_first = 0.f, b_last = 0.f, ibm = 0.f;
         auto band = [&](int e, int &i0, int &i1) {
             const float target = e ? nbf - 1.f : 0.f;
             const float za = (target - edge - p.cb) * ibm, zb = (target + edge - p.cb) * ibm;
-            const float flo = (fminf(za, zb) - p.corner_z) * idz - 0.5f - 1.f / 64;
-            const float fhi = (fmaxf(za, zb) - p.corner_z) * idz - 0.5f + 1.f / 64;
+            const float flo = (fminf(za, zb) - p.corner_z) * idz - 0.5f - 1.f / 1024;
+            const float fhi = (fmaxf(za, zb) - p.corner_z) * idz - 0.5f + 1.f / 1024;
             i0 = max(0, __float2int_ru(fmaxf(flo, -1.f)));
             i1 = min(p.nz - 1, __float2int_rd(fminf(fhi, (float)p.nz)));
         };

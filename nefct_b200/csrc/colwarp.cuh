@@ -150,7 +150,7 @@ __device__ __forceinline__ void col_slab(ColLane &L, float dz, bool zdiv, float 
         s.idx[1] = b1 + ((SPLIT == 2 || vfirst) ? i2 : i1);
         if (CHECK) {
             const bool adm = L.live && (unsigned)cv1 < (unsigned)nv && (unsigned)(cw1 + (int)wx) < (unsigned)(nz + (int)wx);
-            const int mw = vfirst ? cw2 : cw1;
+            const int mw = (SPLIT == 2 || vfirst) ? cw2 : cw1;     // the slot's own voxel
             s.ok[0] = adm && cw1 >= 0;
             s.ok[1] = adm && wx && (unsigned)mw < (unsigned)nz;
         } else {

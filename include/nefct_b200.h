@@ -105,7 +105,8 @@ typedef struct nefct_cb_geom {
 #define NEFCT_TIE_GT        0x01u /* x drives only when |xd| > |yd| (backproject_device :480, cpp/siddon :42) */
 #define NEFCT_SKIP_SHORT    0x02u /* skip rays with hypot(xd, yd) < 10 voxels (Q4: :472, cpp :33,:358) */
 #define NEFCT_NO_INV_L2     0x04u /* weights without 1/L^2: plain line integrals (backproject_device :526) */
-#define NEFCT_Q5            0x08u /* extra 1/L on y-driven three-voxel middle weights (cpp/siddon :292,:313) */
+#define NEFCT_Q5            0x08u /* extra 1/L on y-driven three-voxel middle weights (cpp/siddon :292,:313);
+                                     LOR calls only: the cone-beam calls refuse it (NEFCT_ERR_UNSUPPORTED) */
 #define NEFCT_Q8_INDEX      0x10u /* cylindrical backprojection reads the sinogram at ia + iv*na + ib*na*nb (:830) */
 #define NEFCT_NO_TRANSPOSE  0x20u /* x-driven rays read the x-fastest volume directly: no workspace, slower */
 #define NEFCT_EXACT         0x80u /* classical exact Siddon instead of the reference's slab split: FP64 per-ray

@@ -238,6 +238,16 @@ __global__ void __launch_bounds__(256) lor_key_kernel(const __grid_constant__ Lo
 static const uint32_t kWalkFlags = NEFCT_TIE_GT | NEFCT_SKIP_SHORT | NEFCT_NO_INV_L2 | NEFCT_Q5 |
                                    NEFCT_Q8_INDEX | NEFCT_NO_TRANSPOSE | NEFCT_DETERMINISTIC | NEFCT_EXACT;
 
+// Flags of the cone-beam calls: the walk switches except NEFCT_Q5, a quirk of
+// the LOR projector (cpp/siddon) that no cone-beam walk applies.
+static nefct_status check_cb_flags(uint32_t flags)
+{
+    if (flags & ~kWalkFlags) return fail(NEFCT_ERR_INVALID, "unknown flag bits 0x%x", flags & ~kWalkFlags);
+    if (flags & NEFCT_Q5)
+        return fail(NEFCT_ERR_UNSUPPORTED, "NEFCT_Q5 belongs to the LOR projector; the cone-beam walks do not take it");
+    return NEFCT_OK;
+}
+
 static nefct_status check_grid(const nefct_grid &g)
 {
     if (g.nx < 1 || g.ny < 1 || g.nz < 1)
@@ -406,7 +416,7 @@ static nefct_status cb_forward_impl(const nefct_cb_geom *g, const T *vol, T *sin
     nefct_status st = check_cb_geom(g);
     if (st) return st;
     if (!vol || !sino) return fail(NEFCT_ERR_INVALID, "vol and sino must be non-NULL");
-    if (flags & ~kWalkFlags) return fail(NEFCT_ERR_INVALID, "unknown flag bits 0x%x", flags & ~kWalkFlags);
+    if ((st = check_cb_flags(flags))) return st;
     CBParams<T> *p = new CBParams<T>();
     fill_cb_params(*p, g, flags);
     p->vol = vol;
@@ -464,8 +474,8 @@ size_t cb_fixed_workspace(const nefct_cb_geom *g, uint32_t flags)
 static nefct_status cb_backward_fixed_impl(const nefct_cb_geom *g, const float *sino, float *vol, uint32_t flags,
                                            void *ws, size_t wsb, cudaStream_t s)
 {
-    if (flags & (NEFCT_Q5 | NEFCT_EXACT))
-        return fail(NEFCT_ERR_UNSUPPORTED, "NEFCT_Q5 and NEFCT_EXACT are not available with NEFCT_DETERMINISTIC");
+    if (flags & NEFCT_EXACT)
+        return fail(NEFCT_ERR_UNSUPPORTED, "NEFCT_EXACT is not available with NEFCT_DETERMINISTIC");
     if (!(g->src_det > 0.f)) return fail(NEFCT_ERR_INVALID, "deterministic transpose needs src_det > 0");
     const size_t nvox = (size_t)g->grid.nx * g->grid.ny * g->grid.nz;
     const bool tr = !(flags & NEFCT_NO_TRANSPOSE);
@@ -526,7 +536,7 @@ static nefct_status cb_backward_impl(const nefct_cb_geom *g, const T *sino, T *v
     nefct_status st = check_cb_geom(g);
     if (st) return st;
     if (!vol || !sino) return fail(NEFCT_ERR_INVALID, "vol and sino must be non-NULL");
-    if (flags & ~kWalkFlags) return fail(NEFCT_ERR_INVALID, "unknown flag bits 0x%x", flags & ~kWalkFlags);
+    if ((st = check_cb_flags(flags))) return st;
     if (flags & NEFCT_DETERMINISTIC) {
         if (sizeof(T) != sizeof(float))
             return fail(NEFCT_ERR_UNSUPPORTED, "NEFCT_DETERMINISTIC is available for float32 only");
@@ -707,7 +717,7 @@ static nefct_status cb_forward_static_impl(const nefct_cb_geom *g, const float *
     nefct_status st = check_cb_geom(g);
     if (st) return st;
     if (!vol || !sino) return fail(NEFCT_ERR_INVALID, "vol and sino must be non-NULL");
-    if (flags & ~kWalkFlags) return fail(NEFCT_ERR_INVALID, "unknown flag bits 0x%x", flags & ~kWalkFlags);
+    if ((st = check_cb_flags(flags))) return st;
     const size_t nvox = (size_t)g->grid.nx * g->grid.ny * g->grid.nz;
     const bool tr = !(flags & NEFCT_NO_TRANSPOSE);
     if (tr && nvox > kStaticScratchFloats)

@@ -227,3 +227,17 @@ def test_fdk_quad_workspace_is_checked(nefct_lib):
     st = nefct_lib.nefct_fdk_backproject_ws(C.byref(g), C.c_void_p(256), C.c_void_p(256), 0, C.c_void_p(264),
                                             need, None)
     assert st == _lib.ERR_INVALID and b"aligned" in nefct_lib.nefct_last_error()
+
+
+def test_cone_beam_refuses_lor_only_flag(nefct_lib):
+    """NEFCT_Q5 is a quirk of the LOR projector: the cone-beam calls refuse it
+    before any CUDA call instead of ignoring it."""
+    from nefct_b200 import _lib
+    g = _geom().struct()
+    ws = C.c_void_p(256)
+    for fn in ("nefct_cb_forward", "nefct_cb_backward"):
+        st = getattr(nefct_lib, fn)(C.byref(g), C.c_void_p(256), C.c_void_p(256), _lib.Q5, ws, 1 << 20, None)
+        assert st == _lib.ERR_UNSUPPORTED, fn
+        assert b"LOR" in nefct_lib.nefct_last_error()
+    st = nefct_lib.nefct_cb_forward_noalloc(C.byref(g), C.c_void_p(256), C.c_void_p(256), _lib.Q5, None)
+    assert st == _lib.ERR_UNSUPPORTED

@@ -35,26 +35,60 @@ __device__ __forceinline__ Tap<T> warp_tap(int ix, int iy, int iz, T mx, T my, T
     return t;
 }
 
-template <typename T>
+#ifndef NEFCT_WARP_VPT
+#define NEFCT_WARP_VPT 2
+#endif
+// Voxels per thread of the forward (x-strided by 32, so every load stays
+// coalesced): a thread issues the field reads of all its voxels, then all
+// their tap gathers, before it sums any -- more loads in flight per thread.
+// Measured (fields and image larger than L2): 1 / 2 / 4 / 8 voxels per
+// thread take 0.78 / 0.70 / 0.96 / 1.62 ms at 512^3 (25 / 32 / 64 / 128
+// registers).
+static constexpr int kWarpVpt = NEFCT_WARP_VPT;
+
+template <typename T, int VPT>
 __global__ void __launch_bounds__(256) warp_forward_kernel(const T *__restrict__ img, const T *__restrict__ mx,
                                                            const T *__restrict__ my, const T *__restrict__ mz,
                                                            int nx, int ny, int nz, T *__restrict__ out)
 {
-    const int ix = blockIdx.x * 32 + threadIdx.x, iy = blockIdx.y * 8 + threadIdx.y, iz = blockIdx.z;
-    if (ix >= nx || iy >= ny) return;
-    const int id = ix + iy * nx + iz * nx * ny;
-    const Tap<T> t = warp_tap<T>(ix, iy, iz, mx[id], my[id], mz[id], nx, ny, nz);
-    T v = (T)0;
-    if (t.ok) {
-        const int sy = nx, sz = nx * ny;
-        const T wx2 = t.fx, wx = (T)1 - wx2, wy2 = t.fy, wy = (T)1 - wy2, wz2 = t.fz, wz = (T)1 - wz2;
-        const T *b = img + t.base;
-        v = __ldg(b) * wx * wy * wz + __ldg(b + sz) * wx * wy * wz2 + __ldg(b + sy) * wx * wy2 * wz +
-            __ldg(b + sy + sz) * wx * wy2 * wz2 + __ldg(b + 1) * wx2 * wy * wz +
-            __ldg(b + 1 + sz) * wx2 * wy * wz2 + __ldg(b + 1 + sy) * wx2 * wy2 * wz +
-            __ldg(b + 1 + sy + sz) * wx2 * wy2 * wz2;
+    const int x0 = blockIdx.x * (32 * VPT) + threadIdx.x, iy = blockIdx.y * 8 + threadIdx.y, iz = blockIdx.z;
+    if (iy >= ny) return;
+    const int row = iy * nx + iz * nx * ny;
+    const int sy = nx, sz = nx * ny;
+    Tap<T> t[VPT];
+#pragma unroll
+    for (int k = 0; k < VPT; ++k) {
+        const int ix = x0 + 32 * k;
+        t[k] = ix < nx ? warp_tap<T>(ix, iy, iz, mx[row + ix], my[row + ix], mz[row + ix], nx, ny, nz) : Tap<T>{0};
     }
-    out[id] = v;
+    T c[VPT][8];
+#pragma unroll
+    for (int k = 0; k < VPT; ++k) {
+        const T *b = img + t[k].base;
+        const bool ok = t[k].ok;
+        c[k][0] = ok ? __ldg(b) : (T)0;
+        c[k][1] = ok ? __ldg(b + sz) : (T)0;
+        c[k][2] = ok ? __ldg(b + sy) : (T)0;
+        c[k][3] = ok ? __ldg(b + sy + sz) : (T)0;
+        c[k][4] = ok ? __ldg(b + 1) : (T)0;
+        c[k][5] = ok ? __ldg(b + 1 + sz) : (T)0;
+        c[k][6] = ok ? __ldg(b + 1 + sy) : (T)0;
+        c[k][7] = ok ? __ldg(b + 1 + sy + sz) : (T)0;
+    }
+#pragma unroll
+    for (int k = 0; k < VPT; ++k) {
+        const int ix = x0 + 32 * k;
+        if (ix >= nx) continue;
+        T v = (T)0;
+        if (t[k].ok) {
+            const T wx2 = t[k].fx, wx = (T)1 - wx2, wy2 = t[k].fy, wy = (T)1 - wy2, wz2 = t[k].fz, wz = (T)1 - wz2;
+            v = c[k][0] * wx * wy * wz + c[k][1] * wx * wy * wz2 + c[k][2] * wx * wy2 * wz +
+                c[k][3] * wx * wy2 * wz2 + c[k][4] * wx2 * wy * wz +
+                c[k][5] * wx2 * wy * wz2 + c[k][6] * wx2 * wy2 * wz +
+                c[k][7] * wx2 * wy2 * wz2;
+        }
+        out[row + ix] = v;
+    }
 }
 
 template <typename T>
@@ -176,7 +210,8 @@ static nefct_status warp_forward_impl(const T *img, const T *mx, const T *my, co
     nefct_status st = check_warp(nx, ny, nz);
     if (st) return st;
     if (!img || !mx || !my || !mz || !out) return fail(NEFCT_ERR_INVALID, "NULL buffer");
-    warp_forward_kernel<T><<<dim3((nx + 31) / 32, (ny + 7) / 8, nz), dim3(32, 8), 0, s>>>(img, mx, my, mz, nx, ny, nz, out);
+    warp_forward_kernel<T, kWarpVpt><<<dim3((nx + 32 * kWarpVpt - 1) / (32 * kWarpVpt), (ny + 7) / 8, nz), dim3(32, 8), 0, s>>>(
+        img, mx, my, mz, nx, ny, nz, out);
     NEFCT_CHECK_LAUNCH("warp_forward_kernel");
     return NEFCT_OK;
 }

@@ -427,6 +427,10 @@ __global__ void __launch_bounds__(256) fdk_quad_kernel(const float *__restrict__
 // sectors (measured 7 % faster than 32 x 1 and 16 x 2, 1 % than 4 x 8).
 static constexpr int kTW = 8;
 
+// Voxel centres held in the kernel parameters (x, then y, then z) when the
+// three axes together have at most this many voxels.
+static constexpr int kCtrMax = 6144;
+
 struct BpParams {
     int nx, ny, nz, na, nb, nv0, nvc, first;
     float sx, sy, sz, corner_x, corner_y, corner_z;
@@ -434,6 +438,8 @@ struct BpParams {
     float inv_da, inv_db, cb;         // 1/da, 1/db and nb/2 - bi_p - 0.5, rounded to float
     int cyl, weight;
     float cs[kViewChunk], sn[kViewChunk];
+    int has_ctr;                      // ctr holds every voxel centre (else computed per thread)
+    float ctr[kCtrMax];
 };
 
 // Per view the column part (rotation, magnification m, detector column a,
@@ -494,9 +500,23 @@ __device__ __forceinline__ void bp_weights(const BpParams &p, BpColumn &c)
 }
 
 // Voxel centre along one axis, pixel.cu.cc:116-118 ((i + 0.5) * s / n + c, in double).
-__device__ __forceinline__ float bp_centre(int i, float s, int n, float c)
+__host__ __device__ __forceinline__ float bp_centre(int i, float s, int n, float c)
 {
     return (float)((i + 0.5) * (double)s / n + (double)c);
+}
+// The same from the host-filled table (the host's double arithmetic gives
+// the same values), saving each thread its double divisions per launch.
+__device__ __forceinline__ float bp_cx(const BpParams &p, int i)
+{
+    return p.has_ctr ? p.ctr[i] : bp_centre(i, p.sx, p.nx, p.corner_x);
+}
+__device__ __forceinline__ float bp_cy(const BpParams &p, int i)
+{
+    return p.has_ctr ? p.ctr[p.nx + i] : bp_centre(i, p.sy, p.ny, p.corner_y);
+}
+__device__ __forceinline__ float bp_cz(const BpParams &p, int i)
+{
+    return p.has_ctr ? p.ctr[p.nx + p.ny + i] : bp_centre(i, p.sz, p.nz, p.corner_z);
 }
 
 // Contribution of one voxel at detector row b from the column's taps:
@@ -532,15 +552,15 @@ __global__ void __launch_bounds__(128) fdk_bp_kernel(const __grid_constant__ BpP
     const int iy = (blockIdx.y * 4 + threadIdx.y) * (32 / kTW) + threadIdx.x / kTW;
     const int z0 = blockIdx.z * kZ;
     if (ix >= p.nx || iy >= p.ny) return;
-    const float xc = bp_centre(ix, p.sx, p.nx, p.corner_x);
-    const float yc = bp_centre(iy, p.sy, p.ny, p.corner_y);
+    const float xc = bp_cx(p, ix);
+    const float yc = bp_cy(p, iy);
     float zc[kZ], acc[kZ];
     const size_t plane = (size_t)p.nx * p.ny;
     const size_t col = (size_t)iy * p.nx + ix;
 #pragma unroll
     for (int k = 0; k < kZ; ++k) {
         const int iz = z0 + k;
-        zc[k] = bp_centre(iz, p.sz, p.nz, p.corner_z);
+        zc[k] = bp_cz(p, min(iz, p.nz - 1));
         acc[k] = (!p.first && iz < p.nz) ? vol[iz * plane + col] : 0.f;
     }
     float zabs = 0.f;
@@ -649,12 +669,20 @@ static constexpr int kEdgeSlots = 4;
 __global__ void __launch_bounds__(256) fdk_edge_kernel(const __grid_constant__ BpParams p,
                                                        const float *__restrict__ sino, float *vol)
 {
+    // the view table in shared memory: lanes read different views, which the
+    // parameter bank would serve one address at a time
+    __shared__ float s_cs[kViewChunk], s_sn[kViewChunk];
+    for (int i = threadIdx.x; i < p.nvc; i += blockDim.x) {
+        s_cs[i] = p.cs[i];
+        s_sn[i] = p.sn[i];
+    }
+    __syncthreads();
     const int lane = threadIdx.x & 31;
     const long long colid = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
     if (colid >= (long long)p.nx * p.ny) return;           // uniform across the warp
     const int ix = (int)(colid % p.nx), iy = (int)(colid / p.nx);
-    const float xc = bp_centre(ix, p.sx, p.nx, p.corner_x);
-    const float yc = bp_centre(iy, p.sy, p.ny, p.corner_y);
+    const float xc = bp_cx(p, ix);
+    const float yc = bp_cy(p, iy);
     const float naf = (float)p.na, nbf = (float)p.nb;
     // Width of the bands decided again: the kernel's detector coordinate
     // differs from the reference's by a few ulp of terms of about half the
@@ -665,12 +693,12 @@ __global__ void __launch_bounds__(256) fdk_edge_kernel(const __grid_constant__ B
     const size_t plane = (size_t)p.nx * p.ny;
     float *const vcol = vol + (size_t)iy * p.nx + ix;
     const float idz = (float)p.nz / p.sz;
-    const float z_first = bp_centre(0, p.sz, p.nz, p.corner_z), z_last = bp_centre(p.nz - 1, p.sz, p.nz, p.corner_z);
+    const float z_first = bp_cz(p, 0), z_last = bp_cz(p, p.nz - 1);
     for (int v0 = 0; v0 < p.nvc; v0 += 32) {
         const int v = v0 + lane;
         const bool has = v < p.nvc;
         const int vt = min(v, p.nvc - 1);                  // lanes past the table read its last entry
-        const float cphi = p.cs[vt], sphi = p.sn[vt];
+        const float cphi = s_cs[vt], sphi = s_sn[vt];
         BpColumn c, cr;
         bool col_ours = false, col_ref = false;
         if (has) {
@@ -698,7 +726,7 @@ __global__ void __launch_bounds__(256) fdk_edge_kernel(const __grid_constant__ B
         };
         // correction of voxel iz (0 where the decisions agree)
         auto delta = [&](int iz, bool whole_column) -> float {
-            const float zc = bp_centre(iz, p.sz, p.nz, p.corner_z);
+            const float zc = bp_cz(p, iz);
             const float b = __fmaf_rn(c.bm, zc, p.cb);
             const bool near_row = fabsf(b) < edge || fabsf(b - (nbf - 1.f)) < edge;
             if (!whole_column && !near_row) return 0.f;
@@ -882,6 +910,13 @@ nefct_status nefct_fdk_backproject_ws(const nefct_cb_geom *g, const float *filte
     p->cb = (float)((double)(g->nb / 2) - (double)p->bi_p - 0.5);
     p->cyl = g->det_kind == NEFCT_DET_CYL;
     p->weight = !(flags & NEFCT_FDK_NO_WEIGHT);
+    p->has_ctr = (long long)g->grid.nx + g->grid.ny + g->grid.nz <= kCtrMax;
+    if (p->has_ctr) {
+        float *c = p->ctr;
+        for (int i = 0; i < p->nx; ++i) *c++ = bp_centre(i, p->sx, p->nx, p->corner_x);
+        for (int i = 0; i < p->ny; ++i) *c++ = bp_centre(i, p->sy, p->ny, p->corner_y);
+        for (int i = 0; i < p->nz; ++i) *c++ = bp_centre(i, p->sz, p->nz, p->corner_z);
+    }
     cudaStream_t s = (cudaStream_t)stream;
     dim3 grid((g->grid.nx + kTW - 1) / kTW, (g->grid.ny + 4 * (32 / kTW) - 1) / (4 * (32 / kTW)), (g->grid.nz + kZ - 1) / kZ);
     const int chunk = quad ? fdk_view_chunk(g->na, g->nb, sizeof(float4)) : fdk_view_chunk(g->na, g->nb);

@@ -297,7 +297,9 @@ nefct_status nefct_fdk_backproject(const nefct_cb_geom *g, const float *filtered
  * 16-byte aligned; NULL gives nefct_fdk_backproject): each chunk of views
  * is first repacked into tap quads (the four bilinear taps of every detector
  * cell side by side) so a voxel reads its taps with one 16-byte load.  Same
- * arithmetic, bit-identical result.  No counterpart in the reference. */
+ * arithmetic, bit-identical result.  The workspace holds one chunk: up to
+ * 128 views, about 400 MB at most (16 bytes per detector cell and view).
+ * No counterpart in the reference. */
 size_t nefct_fdk_workspace_bytes(const nefct_cb_geom *g);
 nefct_status nefct_fdk_backproject_ws(const nefct_cb_geom *g, const float *filtered, float *vol, uint32_t flags,
                                       void *ws, size_t ws_bytes, void *stream);

@@ -390,15 +390,16 @@ static cudaError_t launch_filter(const FilterParams &p, const float *sino, float
 #define NEFCT_FDK_KZ 8
 #endif
 static constexpr int kZ = NEFCT_FDK_KZ;
-// Views per launch: as many as keep a chunk of filtered projections within
-// ~52 MB (an L2-resident chunk beside an L2-resident 256^3 volume), 8 to 64
-// (64 for 512 x 384 detectors; measured 1 % faster than 48, 3 % than 32 and
-// 8 % than 16: fewer read-modify-write passes over the volume).
-static constexpr int kViewChunk = 64;
+// Views per launch: as many as fit ~400 MB of a chunk (tap quads: 16 bytes
+// per detector cell), 8 to 128.  Fewer launches mean fewer read-modify-write
+// passes over the volume and fewer launch tails; that outweighs keeping the
+// chunk L2-resident (256^3, 360 views of 512 x 384 with quads: 17 / 32 / 64
+// / 128 views per launch take 7.56 / 7.26 / 7.07 / 6.98 ms).
+static constexpr int kViewChunk = 128;
 static inline int fdk_view_chunk(int na, int nb, size_t bytes_per_cell = sizeof(float))
 {
     const double per_view = (double)na * nb * bytes_per_cell;
-    return (int)std::min<double>(kViewChunk, std::max<double>(8.0, (double)(52 << 20) / per_view));
+    return (int)std::min<double>(kViewChunk, std::max<double>(8.0, (double)(400 << 20) / per_view));
 }
 
 // Tap quads: for a chunk of views, quad[(v * nb + ib) * na + ia] holds the

@@ -441,7 +441,7 @@ def run_gpu(args):
     peak, peak_kind = load_peaks()
     fwd_s, bwd_s = t_fwd / args.steps, t_bwd / args.steps
     walk = tuned["walk"]
-    names = {"fwd": "cb_colwarp_kernel<forward>" if walk & 1 else "cb_forward_kernel",
+    names = {"fwd": "cb_colwarp_rows_kernel<forward>" if walk & 1 else "cb_forward_kernel",
              "bwd": "cb_colwarp_kernel<transpose>" if walk & 2 else "cb_backward_kernel"}
     traffic = load_traffic(args.workload)
     issue = load_issue(args.workload)

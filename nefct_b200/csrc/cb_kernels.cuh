@@ -9,7 +9,8 @@
 //    rays;
 //  * column warps (cb_colwarp_kernel, FP32): each warp 32 consecutive rows
 //    of one column, blockDim.y columns per CTA, over a z-fastest copy of the
-//    volume (colwarp.cuh).
+//    volume (colwarp.cuh); the forward's cb_colwarp_rows_kernel gives each
+//    lane two rows (l and l + 32) of a 64-row tile.
 // The grid runs (column tile, view, row band) with the row band slowest, or
 // (column tile, row band, view).  Per-view cos/sin/z-offset ride in the
 // kernel parameters.
@@ -165,6 +166,83 @@ __device__ __forceinline__ void colwarp_lane(const GridDev<float> &g, const floa
     }
 }
 
+// R rays per lane (rows l, l + 32, ... of the column): the same walk and
+// arithmetic per ray as colwarp_lane, with the warp's slab table and split
+// decisions shared by all 32 R rays.  Float forward (FWD) and float
+// transpose only.
+template <bool DIV, bool FWD, int R>
+__device__ __forceinline__ void colwarp_rows(const GridDev<float> &g, const float (&r)[R][6], const bool (&has)[R],
+                                             uint32_t flags, const float *__restrict__ volZ, float *const (&out)[R],
+                                             const float (&y)[R], float *accZ)
+{
+    Walk<float> w[R];
+    bool live[R];
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        w[k] = Walk<float>{};
+        live[k] = has[k] && (FWD || y[k] != 0.f) && setup_walk(g, r[k], flags, w[k]);
+        any = any || live[k];
+    }
+    if (!__any_sync(0xffffffffu, any)) {
+        if (FWD) {
+#pragma unroll
+            for (int k = 0; k < R; ++k)
+                if (has[k]) *out[k] = 0.f;
+        }
+        return;
+    }
+    ColShared c;
+    ColLane L[R];
+    int K0, K1, KI0, KI1;
+    if (!col_setup_rows<R>(g, w, live, c, L, K0, K1, KI0, KI1)) {
+        // rays of the column disagree on the shared parameters: each walks alone
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            unsigned su, sv;
+            col_strides(g, w[k].xdrive, su, sv);
+            if (FWD) {
+                const float v = live[k] ? gather_walk<float, DIV, false, false>(w[k], g, volZ, (int)su, (int)sv, 1) : 0.f;
+                if (has[k]) *out[k] = v;
+            } else if (live[k]) {
+                scatter_walk<float, DIV, false, false>(w[k], g, accZ, (int)su, (int)sv, 1, y[k]);
+            }
+        }
+        return;
+    }
+    if constexpr (FWD) {
+        float acc[R];
+#pragma unroll
+        for (int k = 0; k < R; ++k) acc[k] = 0.f;
+        auto f = [&](const auto &s, int k) {
+            float v[s.n];
+#pragma unroll
+            for (int i = 0; i < s.n; ++i) v[i] = (!s.checked || s.ok[i]) ? __ldg(volZ + s.idx[i]) : 0.f;
+#pragma unroll
+            for (int i = 0; i < s.n; ++i) acc[k] += v[i] * s.r[i];
+        };
+        col_walk_any_rows<DIV, 0, R>(c, L, K0, K1, KI0, KI1, g, f);
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+            if (has[k]) *out[k] = live[k] ? acc[k] * w[k].W : 0.f;
+    } else {
+        float yw[R];
+#pragma unroll
+        for (int k = 0; k < R; ++k) yw[k] = y[k] * w[k].W;
+        auto f = [&](const auto &s, int k) {
+            if constexpr (s.n == 2) {
+                if (s.ok[0]) atomicAdd(accZ + s.idx[0], yw[k] * s.r[0]);
+                if (s.ok[1]) atomicAdd(accZ + s.idx[1], fmaf(-yw[k], s.r[0], yw[k]));
+            } else {
+#pragma unroll
+                for (int i = 0; i < s.n; ++i)
+                    if (s.ok[i]) atomicAdd(accZ + s.idx[i], yw[k] * s.r[i]);
+            }
+        };
+        col_walk_any_rows<DIV, 2, R>(c, L, K0, K1, KI0, KI1, g, f);
+    }
+}
+
 // Column warps: warp = rows [32*tile, 32*tile + 32) of column ia at view iv,
 // over the z-fastest copy p.volT (forward, into p.out) or accumulator p.outT.
 // (at most 64 registers: 4 CTAs of 256 threads per SM; measured faster than
@@ -187,6 +265,46 @@ __global__ void __launch_bounds__(256, 4) cb_colwarp_kernel(const __grid_constan
     colwarp_lane<DIV, FWD>(p.g, r, has, p.flags, p.volT, out, y, p.outT);
 }
 
+// Rays per lane of the float column-warp kernels, per direction.  Measured
+// (512^3, 180 of 720 views of 1024 x 768; 256^3, 360 views of 512 x 384):
+// two rays per lane take the forward from 79.6 to 77.7 ms and from 19.1 to
+// 18.8 ms (80 registers, 3 CTAs of 256 per SM; bit-identical output) but
+// the transpose from 97.8 to 100.2 ms, so the transpose keeps one.
+#ifndef NEFCT_COL_ROWS_FWD
+#define NEFCT_COL_ROWS_FWD 2
+#endif
+#ifndef NEFCT_COL_ROWS_BWD
+#define NEFCT_COL_ROWS_BWD 1
+#endif
+#ifndef NEFCT_COL_MINB
+#define NEFCT_COL_MINB 3
+#endif
+
+// Column warps with R rays per lane: warp = rows [32 R tile, 32 R (tile + 1))
+// of column ia at view iv (at most 80 registers: 3 CTAs of 256 per SM).
+template <bool DIV, bool FWD, int R>
+__global__ void __launch_bounds__(256, NEFCT_COL_MINB) cb_colwarp_rows_kernel(const __grid_constant__ CBParams<float> p)
+{
+    const int lane = threadIdx.x;
+    const int ia = blockIdx.x * blockDim.y + threadIdx.y;
+    const int tile = p.band_major ? blockIdx.z : blockIdx.y;
+    const int iv = p.band_major ? blockIdx.y : blockIdx.z;
+    if (ia >= p.na) return;                       // uniform across the warp
+    float r[R][6];
+    bool has[R];
+    float y[R];
+    float *out[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        const int ib = (tile * R + k) * 32 + lane;
+        has[k] = ib < p.nb;
+        y[k] = (!FWD && has[k]) ? cb_sino_value(p, ia, ib, iv) : 0.f;
+        cb_ray(p, ia, has[k] ? ib : 0, iv, r[k]);
+        out[k] = FWD ? p.out + (size_t)(p.v0 + iv) * p.na * p.nb + (size_t)ib * p.na + ia : nullptr;
+    }
+    colwarp_rows<DIV, FWD, R>(p.g, r, has, p.flags, p.volT, out, y, p.outT);
+}
+
 // Launch shape of the thread walk for nvc views (see cb_cell).
 template <typename T>
 static inline void cb_shape(CBParams<T> &p, int na, int nb, int nvc, dim3 &grid, dim3 &block)
@@ -201,12 +319,13 @@ static inline void cb_shape(CBParams<T> &p, int na, int nb, int nvc, dim3 &grid,
 // Launch shape of the column warps: NEFCT_TUNE_CB_ROWS columns (warps) per
 // CTA, 32 rows per warp.
 template <typename T>
-static inline void cb_colwarp_shape(CBParams<T> &p, int na, int nb, int nvc, dim3 &grid, dim3 &block)
+static inline void cb_colwarp_shape(CBParams<T> &p, int na, int nb, int nvc, dim3 &grid, dim3 &block,
+                                    int rays_per_lane = 1)
 {
     const int cols = tune_get(NEFCT_TUNE_CB_ROWS);
     p.band_major = tune_get(NEFCT_TUNE_CB_ORDER) == 0;
     block = dim3(32, cols);
-    const unsigned tiles = (unsigned)((nb + 31) / 32);
+    const unsigned tiles = (unsigned)((nb + 32 * rays_per_lane - 1) / (32 * rays_per_lane));
     grid = p.band_major ? dim3((na + cols - 1) / cols, nvc, tiles) : dim3((na + cols - 1) / cols, tiles, nvc);
 }
 
@@ -247,9 +366,16 @@ template <bool FWD>
 static inline cudaError_t cb_launch_colwarp(CBParams<float> &p, int na, int nb, int nvc, cudaStream_t s)
 {
     dim3 grid, block;
-    cb_colwarp_shape(p, na, nb, nvc, grid, block);
-    if (cubic(p.g)) cb_colwarp_kernel<false, FWD><<<grid, block, 0, s>>>(p);
-    else cb_colwarp_kernel<true, FWD><<<grid, block, 0, s>>>(p);
+    constexpr int R = FWD ? NEFCT_COL_ROWS_FWD : NEFCT_COL_ROWS_BWD;
+    if constexpr (R > 1) {
+        cb_colwarp_shape(p, na, nb, nvc, grid, block, R);
+        if (cubic(p.g)) cb_colwarp_rows_kernel<false, FWD, R><<<grid, block, 0, s>>>(p);
+        else cb_colwarp_rows_kernel<true, FWD, R><<<grid, block, 0, s>>>(p);
+    } else {
+        cb_colwarp_shape(p, na, nb, nvc, grid, block);
+        if (cubic(p.g)) cb_colwarp_kernel<false, FWD><<<grid, block, 0, s>>>(p);
+        else cb_colwarp_kernel<true, FWD><<<grid, block, 0, s>>>(p);
+    }
     return cudaGetLastError();
 }
 

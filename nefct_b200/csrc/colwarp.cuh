@@ -115,17 +115,13 @@ template <int NS, bool CHK> struct ColSlots {
 // with the second slot always at w2 (it differs from the reference's pairing
 // only when the ratio rounds to 1 or above, where that slot's weight is a
 // rounding error; for the float transpose, whose atomic sums are not
-// reproducible anyway).  f(slots) consumes.
-template <bool DIV, bool CHECK, int WUP, int SPLIT, class Fn>
-__device__ __forceinline__ void col_slab(ColLane &L, float dz, bool zdiv, float nz2, int nv, int nz,
-                                         const ColTable &tab, int j, Fn &f)
+// reproducible anyway).  f(slots) consumes.  The slab's table entry (b1,
+// b2, exit plane offset d, v ratio rv, packed v floors cv) comes from the
+// caller; TWO: the two-slot split (the caller's SPLIT and no v crossing).
+template <bool DIV, bool CHECK, int WUP, int SPLIT, bool TWO, class Fn>
+__device__ __forceinline__ void col_lane_slab(ColLane &L, float dz, bool zdiv, float nz2, int nv, int nz,
+                                              unsigned b1, unsigned b2, float d, float rv, unsigned cv, Fn &f)
 {
-    const uint4 te = tab.e[j];          // same address for every lane: one broadcast
-    const unsigned b1 = te.x, b2 = te.y;
-    const float d = __uint_as_float(te.w);
-    unsigned cv = 0;
-    if (CHECK) cv = tab.cv[j];
-
     float qbw = __fadd_rn(L.pw, __fmul_rn(L.kw, d));
     if (DIV && zdiv) qbw = __fdiv_rn(qbw, dz);
     qbw = __fadd_rn(qbw, nz2);
@@ -140,7 +136,7 @@ __device__ __forceinline__ void col_slab(ColLane &L, float dz, bool zdiv, float 
     const unsigned i1 = (unsigned)__float_as_int(m1w), i2 = (unsigned)__float_as_int(m2w);
     const int cv1 = CHECK ? (int)(cv & 0xffffu) - 2 : 0, cv2 = CHECK ? (int)(cv >> 16) - 2 : 0;
     const int cw1 = (int)i1 - kFloorMagicBits, cw2 = (int)i2 - kFloorMagicBits;
-    if (SPLIT && b1 == b2) {
+    if constexpr (TWO) {
         // no v crossing (uniform across the warp)
         const bool vfirst = 1.f > rw;
         ColSlots<2, CHECK> s;
@@ -159,7 +155,6 @@ __device__ __forceinline__ void col_slab(ColLane &L, float dz, bool zdiv, float 
         }
         f(s);
     } else {
-        const float rv = __uint_as_float(te.z);
         const bool vx = SPLIT || b1 != b2;
         const bool vfirst = rv > rw;
         ColSlots<3, CHECK> s;
@@ -183,6 +178,46 @@ __device__ __forceinline__ void col_slab(ColLane &L, float dz, bool zdiv, float 
             s.ok[2] = L.live && vx && wx;
         }
         f(s);
+    }
+}
+
+// One slab of the lane's one ray, its entry read from the warp's table.
+template <bool DIV, bool CHECK, int WUP, int SPLIT, class Fn>
+__device__ __forceinline__ void col_slab(ColLane &L, float dz, bool zdiv, float nz2, int nv, int nz,
+                                         const ColTable &tab, int j, Fn &f)
+{
+    const uint4 te = tab.e[j];          // same address for every lane: one broadcast
+    const unsigned cv = CHECK ? tab.cv[j] : 0u;
+    if (SPLIT && te.x == te.y)
+        col_lane_slab<DIV, CHECK, WUP, SPLIT, true>(L, dz, zdiv, nz2, nv, nz, te.x, te.y, __uint_as_float(te.w),
+                                                    __uint_as_float(te.z), cv, f);
+    else
+        col_lane_slab<DIV, CHECK, WUP, SPLIT, false>(L, dz, zdiv, nz2, nv, nz, te.x, te.y, __uint_as_float(te.w),
+                                                     __uint_as_float(te.z), cv, f);
+}
+
+// The same slab for the R rays of a lane (rows l, l + 32, ... of the
+// column): one table read and one split decision for all of them;
+// f(slots, r) consumes ray r's slots.
+template <bool DIV, bool CHECK, int WUP, int SPLIT, int R, class Fn>
+__device__ __forceinline__ void col_slab_rows(ColLane (&L)[R], float dz, bool zdiv, float nz2, int nv, int nz,
+                                              const ColTable &tab, int j, Fn &f)
+{
+    const uint4 te = tab.e[j];
+    const unsigned cv = CHECK ? tab.cv[j] : 0u;
+    const float d = __uint_as_float(te.w), rv = __uint_as_float(te.z);
+    if (SPLIT && te.x == te.y) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            auto fr = [&](const auto &s) { f(s, r); };
+            col_lane_slab<DIV, CHECK, WUP, SPLIT, true>(L[r], dz, zdiv, nz2, nv, nz, te.x, te.y, d, rv, cv, fr);
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            auto fr = [&](const auto &s) { f(s, r); };
+            col_lane_slab<DIV, CHECK, WUP, SPLIT, false>(L[r], dz, zdiv, nz2, nv, nz, te.x, te.y, d, rv, cv, fr);
+        }
     }
 }
 
@@ -282,6 +317,125 @@ __device__ __forceinline__ bool col_setup(const GridDev<float> &g, const Walk<fl
     L.kw = live ? w.kw : 0.f;
     L.live = live;
     L.up = w.kw >= 0.f;
+    return true;
+}
+
+// ---- R rays per lane: rows l, l + 32, ..., l + 32 (R - 1) of the column ----
+//
+// The warp's table serves 32 R rays: each slab's entry is read and its split
+// decided once per lane for all of them.  Each ray's own arithmetic is the
+// one-ray walk's.
+
+template <bool DIV, bool CHECK, int WUP, int SPLIT, int R, class Fn>
+__device__ __forceinline__ void col_range_rows(int a, int b, int kc, const ColShared &c, ColLane (&L)[R],
+                                               const ColTable &tab, const GridDev<float> &g, Fn &f)
+{
+    const bool zdiv = g.dz != 1.f;
+#pragma unroll 2
+    for (int k = a; k <= b; ++k)
+        col_slab_rows<DIV, CHECK, WUP, SPLIT, R>(L, g.dz, zdiv, g.nz2, c.nv, g.nz, tab, k - kc, f);
+}
+
+template <bool DIV, int WUP, int SPLIT, int R, class Fn>
+__device__ __forceinline__ void col_walk_rows(const ColShared &c, ColLane (&L)[R], int K0, int K1, int KI0, int KI1,
+                                              const GridDev<float> &g, ColTable &tab, Fn &f)
+{
+    const float t = __fsub_rn((float)K0, c.nu2);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        float q = __fadd_rn(L[r].pw, __fmul_rn(L[r].kw, __fsub_rn(t, c.pu)));
+        if (DIV && g.dz != 1.f) q = __fdiv_rn(q, g.dz);
+        L[r].qaw = __fadd_rn(q, g.nz2);
+        L[r].maw = magic_floor<true>(L[r].qaw);
+    }
+    const int lane = threadIdx.x & 31;
+    if (KI0 > KI1) { KI0 = K1 + 1; KI1 = K1; }
+    for (int kc = K0; kc <= K1; kc += 32) {
+        const ColEntry e = col_entry<DIV>(c, kc + lane);
+        const float d = __fsub_rn(__fadd_rn(__fsub_rn((float)(kc + lane), c.nu2), 1.f), c.pu);
+        __syncwarp();
+        tab.e[lane] = make_uint4(e.b1, e.b2, __float_as_uint(e.rv), __float_as_uint(d));
+        tab.cv[lane] = e.cv;
+        __syncwarp();
+        const int ke = min(K1, kc + 31);
+        col_range_rows<DIV, true, WUP, SPLIT, R>(kc, min(ke, KI0 - 1), kc, c, L, tab, g, f);
+        col_range_rows<DIV, false, WUP, SPLIT, R>(max(kc, KI0), min(ke, KI1), kc, c, L, tab, g, f);
+        col_range_rows<DIV, true, WUP, SPLIT, R>(max(kc, KI1 + 1), ke, kc, c, L, tab, g, f);
+    }
+}
+
+template <bool DIV, int SPLIT, int R, class Fn>
+__device__ __forceinline__ void col_walk_any_rows(const ColShared &c, ColLane (&L)[R], int K0, int K1, int KI0,
+                                                  int KI1, const GridDev<float> &g, Fn &f)
+{
+    __shared__ ColTable tables[8];
+    ColTable &tab = tables[threadIdx.y];
+    bool up = true, down = true;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        up = up && (L[r].up || !L[r].live);
+        down = down && (!L[r].up || !L[r].live);
+    }
+    const bool all_up = __all_sync(0xffffffffu, up), all_down = __all_sync(0xffffffffu, down);
+    if (all_up) col_walk_rows<DIV, 1, SPLIT, R>(c, L, K0, K1, KI0, KI1, g, tab, f);
+    else if (all_down) col_walk_rows<DIV, 0, SPLIT, R>(c, L, K0, K1, KI0, KI1, g, tab, f);
+    else col_walk_rows<DIV, 2, SPLIT, R>(c, L, K0, K1, KI0, KI1, g, tab, f);
+}
+
+// col_setup for R rays per lane (all in one detector column).
+template <int R>
+__device__ __forceinline__ bool col_setup_rows(const GridDev<float> &g, const Walk<float> (&w)[R],
+                                               const bool (&live)[R], ColShared &c, ColLane (&L)[R], int &K0,
+                                               int &K1, int &KI0, int &KI1)
+{
+    bool any = false;
+    int first = 0;
+#pragma unroll
+    for (int r = R - 1; r >= 0; --r)
+        if (live[r]) { any = true; first = r; }
+    float pu = w[0].pu, pv = w[0].pv, kv = w[0].kv;
+    bool xd = w[0].xdrive;
+#pragma unroll
+    for (int r = 1; r < R; ++r)
+        if (first == r) { pu = w[r].pu; pv = w[r].pv; kv = w[r].kv; xd = w[r].xdrive; }
+    const unsigned lm = __ballot_sync(0xffffffffu, any);
+    const int src = __ffs(lm) - 1;
+    c.pu = __shfl_sync(0xffffffffu, pu, src);
+    c.pv = __shfl_sync(0xffffffffu, pv, src);
+    c.kv = __shfl_sync(0xffffffffu, kv, src);
+    const bool xdrive = __shfl_sync(0xffffffffu, (int)xd, src) != 0;
+    bool same = true;
+    int k0 = INT_MAX, k1 = INT_MIN, ki0 = INT_MIN, ki1 = INT_MAX;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        same = same && (!live[r] || (__float_as_int(w[r].pu) == __float_as_int(c.pu) &&
+                                     __float_as_int(w[r].pv) == __float_as_int(c.pv) &&
+                                     __float_as_int(w[r].kv) == __float_as_int(c.kv) && w[r].xdrive == xdrive));
+        if (live[r]) {
+            k0 = min(k0, w[r].k0);
+            k1 = max(k1, w[r].k1);
+            ki0 = max(ki0, w[r].ki0);
+            ki1 = min(ki1, w[r].ki1);
+        }
+    }
+    if (!__all_sync(0xffffffffu, same)) return false;
+    c.dv = xdrive ? g.dy : 1.f;
+    c.vdiv = xdrive && g.dy != 1.f;
+    c.nv2 = xdrive ? g.ny2 : g.nx2;
+    c.nu2 = xdrive ? g.nx2 : g.ny2;
+    c.nv = xdrive ? g.ny : g.nx;
+    col_strides(g, xdrive, c.su, c.sv);
+    K0 = __reduce_min_sync(0xffffffffu, k0);
+    K1 = __reduce_max_sync(0xffffffffu, k1);
+    KI0 = __reduce_max_sync(0xffffffffu, ki0);
+    KI1 = __reduce_min_sync(0xffffffffu, ki1);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        L[r].pw = live[r] ? w[r].pw : 0.f;
+        L[r].kw = live[r] ? w[r].kw : 0.f;
+        L[r].live = live[r];
+        L[r].up = w[r].kw >= 0.f;
+    }
     return true;
 }
 
